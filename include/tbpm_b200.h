@@ -1,0 +1,208 @@
+/*
+ * tbpm_b200.h -- C ABI of libtbpm_b200.so, the B200 (sm_100a) replacement of
+ * the TBPM numeric core of TBPLaS (deepmodeling/tbplas 1.6.0), i.e. of the f2py
+ * extension module `tbplas.fortran.f2py` built from tbplas/fortran/tbpm.f90.
+ *
+ * Conventions
+ *  - Only plain C types cross this boundary.  Complex numbers are interleaved
+ *    (re, im) doubles, exactly as numpy complex128 lays them out.
+ *  - CSR arrays are 0-based (indptr[n_rows+1], indices[nnz], hop[nnz] complex),
+ *    the layout produced by tbplas Sample.build_ham_csr / build_ham_dxy after
+ *    f2py's cast of the index arrays to int32 (csr.F90:20-24).
+ *  - Multi-dimensional outputs use the Fortran (column-major) layout that f2py
+ *    returns, so a caller can wrap them with numpy order='F' unchanged.
+ *  - Every function returns a status code (TBPM_OK on success); on failure
+ *    tbpm_last_error() describes the problem.  The library never exits the
+ *    process and never traps the GPU.  Where the reference Fortran calls
+ *    `stop` (funcs.f90:175-192 check_norm) this library returns TBPM_ERR_NORM.
+ *  - The random initial states of the reference come from gfortran's intrinsic
+ *    RANDOM_NUMBER, which cannot be reproduced; this library draws the same
+ *    distribution (random.f90:36-69) from a Philox4x32-10 stream keyed by the
+ *    same seed rule (tbpm.f90:57).  The *_states entry points take the initial
+ *    states from the caller instead.
+ *  - Calls on one context are serialised on the context's CUDA stream.
+ */
+#ifndef TBPM_B200_H
+#define TBPM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define TBPM_OK 0
+#define TBPM_ERR_ARG 1     /* invalid argument (shape, size, range) */
+#define TBPM_ERR_NORM 2    /* wave-function norm check failed (check_norm) */
+#define TBPM_ERR_NAN 3     /* NaN / Inf detected */
+#define TBPM_ERR_CUDA 4    /* CUDA runtime error */
+#define TBPM_ERR_TIMEOUT 5 /* a bounded device-side wait expired */
+#define TBPM_ERR_OOM 6     /* device allocation failed */
+#define TBPM_ERR_STATE 7   /* call out of order (e.g. no Hamiltonian uploaded) */
+
+/* arithmetic of the propagation */
+#define TBPM_PREC_FP64 0 /* complex128 states, SpMV and reductions */
+#define TBPM_PREC_FP32 1 /* complex64 states and SpMV; FP64 coefficients,
+                            rescaling and correlation reductions */
+
+/* random initial state distributions */
+#define TBPM_STATE_EXP 0  /* |z|^2 ~ Exp(1), phase ~ U[0,2pi) (random.f90:36-69) */
+#define TBPM_STATE_UNIT 1 /* |z| = 1, phase ~ U[0,2pi) */
+
+typedef struct tbpm_ctx tbpm_ctx;
+
+typedef struct tbpm_options {
+  int precision;         /* TBPM_PREC_FP64 (default) or TBPM_PREC_FP32 */
+  int batch;             /* states propagated together as one block; 0 = 16 */
+  int state_kind;        /* TBPM_STATE_EXP (default) or TBPM_STATE_UNIT */
+  int verbose;           /* 1: print progress like the reference on rank 0 */
+  int threads_per_block; /* 0 = tuned default */
+  int rows_per_tile;     /* 0 = tuned default */
+  int steps_per_graph;   /* time steps captured per CUDA graph; 0 = 16 */
+  int use_graphs;        /* 1 (default): replay captured CUDA graphs */
+  double fp32_chk_thr;   /* lower bound of the norm-check threshold in FP32
+                            mode (default 1e-4); FP64 uses wfn_chk_thr as is */
+} tbpm_options;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Create a context on CUDA device `device` with its own non-blocking stream. */
+int tbpm_create(int device, tbpm_ctx** ctx);
+int tbpm_destroy(tbpm_ctx* ctx);
+const char* tbpm_last_error(const tbpm_ctx* ctx);
+int tbpm_set_options(tbpm_ctx* ctx, const tbpm_options* opts);
+int tbpm_get_options(const tbpm_ctx* ctx, tbpm_options* opts);
+/* The cudaStream_t (as void*) all work of the context is enqueued on. */
+void* tbpm_get_stream(const tbpm_ctx* ctx);
+/* Statistics of the last propagation: kernel launches enqueued and the model
+ * of algorithmic HBM bytes they move (see DESIGN.md of the source tree). */
+int tbpm_last_stats(const tbpm_ctx* ctx, int64_t* kernel_launches, double* model_bytes);
+int tbpm_version(void);
+
+/* ---- resident Hamiltonian ------------------------------------------------ */
+
+/* Upload a CSR Hamiltonian (host arrays) to the device in the context's
+ * precision.  dx, dy (float64[nnz]) are optional (NULL) and needed by the AC
+ * and DC drivers; `rescale` is Sample.rescale (used for the current operator,
+ * funcs.f90:12-33).  Replaces make_csr_matrix (csr.F90:45-68). */
+int tbpm_ham_upload(tbpm_ctx* ctx, const int32_t* indptr, const int32_t* indices,
+                    const double* hop, int64_t n_rows, int64_t nnz, const double* dx,
+                    const double* dy, double rescale);
+int tbpm_ham_release(tbpm_ctx* ctx);
+
+/* ---- f2py-equivalent drivers (host buffers in, host buffers out) --------- */
+
+/* tbpm_dos -- replaces tbpm.f90:6-93 (SUBROUTINE tbpm_dos) as called from
+ * Solver.calc_corr_dos (tbpm/solver.py:256-284).
+ * corr: complex128[n_timestep + 1].  Uses the uploaded Hamiltonian when
+ * indptr == NULL, otherwise uploads (indptr, indices, hop) first. */
+int tbpm_dos(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+             const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+             int seed, int n_timestep, int n_ran_samples, int rank, int wfn_chk_step,
+             double wfn_chk_thr, double* corr);
+
+/* As tbpm_dos with caller-supplied initial states wf0 (complex128
+ * [n_states][n_rows], C order).  corr_per_state (optional, complex128
+ * [n_states][n_timestep + 1]) receives the unaveraged correlations. */
+int tbpm_dos_states(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+                    const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+                    const double* wf0, int n_states, int n_timestep, int wfn_chk_step,
+                    double wfn_chk_thr, double* corr, double* corr_per_state);
+
+/* tbpm_accond -- replaces tbpm.f90:193-351 (SUBROUTINE tbpm_accond) as called
+ * from Solver.calc_corr_ac_cond (tbpm/solver.py:317-352).
+ * corr: complex128 (4, n_timestep) Fortran order (xx, xy, yx, yy); column 1
+ * (t = 1) is zero as in the reference. */
+int tbpm_accond(tbpm_ctx* ctx, const double* bes, int n_bes, double beta, double mu,
+                const int32_t* indptr, const int32_t* indices, const double* hop,
+                int64_t n_rows, int64_t nnz, double h_rescale, const double* dx,
+                const double* dy, int seed, int n_timestep, int n_ran_samples, int nr_fermi,
+                double fermi_precision, int rank, int wfn_chk_step, double wfn_chk_thr,
+                double* corr);
+
+/* As tbpm_accond with caller-supplied initial states (complex128 [n_states][n_rows]). */
+int tbpm_accond_states(tbpm_ctx* ctx, const double* bes, int n_bes, double beta, double mu,
+                       const int32_t* indptr, const int32_t* indices, const double* hop,
+                       int64_t n_rows, int64_t nnz, double h_rescale, const double* dx,
+                       const double* dy, const double* wf0, int n_states, int n_timestep,
+                       int nr_fermi, double fermi_precision, int wfn_chk_step,
+                       double wfn_chk_thr, double* corr);
+
+/* tbpm_dccond -- replaces tbpm.f90:497-718 (SUBROUTINE tbpm_dccond) as called
+ * from Solver.calc_corr_dc_cond (tbpm/solver.py:393-441).
+ * dos_corr: complex128[n_timestep]; dc_corr: complex128 (2, n_energies,
+ * n_timestep) Fortran order, the first n_en_inds rows of the energy axis
+ * filled (as in the reference). */
+int tbpm_dccond(tbpm_ctx* ctx, const double* bes, int n_bes, double beta, double mu,
+                const int32_t* indptr, const int32_t* indices, const double* hop,
+                int64_t n_rows, int64_t nnz, double h_rescale, const double* dx,
+                const double* dy, int seed, int n_timestep, int n_ran_samples, double t_step,
+                const double* energies, int n_energies, const int32_t* en_inds,
+                int n_en_inds, int rank, int wfn_chk_step, double wfn_chk_thr,
+                double* dos_corr, double* dc_corr);
+
+/* As tbpm_dccond with caller-supplied initial states (complex128 [n_states][n_rows]). */
+int tbpm_dccond_states(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+                       const int32_t* indices, const double* hop, int64_t n_rows,
+                       int64_t nnz, double h_rescale, const double* dx, const double* dy,
+                       const double* wf0, int n_states, int n_timestep, double t_step,
+                       const double* energies, int n_energies, const int32_t* en_inds,
+                       int n_en_inds, int wfn_chk_step, double wfn_chk_thr,
+                       double* dos_corr, double* dc_corr);
+
+/* tbpm_psi_t -- replaces tbpm.f90:1029-1093 (SUBROUTINE tbpm_psi_t) as called
+ * from Solver.calc_psi_t (tbpm/solver.py:543-600).
+ * psi0: complex128[n_rows]; time_log: int32[n_time_log] sorted, unique, in
+ * [0, n_timestep]; psi_t: complex128 (n_rows, n_time_log) Fortran order. */
+int tbpm_psi_t(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+               const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+               const double* psi0, const int32_t* time_log, int n_time_log, int n_timestep,
+               int wfn_chk_step, double wfn_chk_thr, double* psi_t);
+
+/* ---- building blocks ----------------------------------------------------- */
+
+/* Random initial states of the reference distribution (random.f90:36-69) with
+ * the seed rule iseed = seed*(first_sample + i + rank*n_ran_samples) for
+ * i = 0..n_states-1 (tbpm.f90:57, first_sample is 1-based).
+ * wf: complex128 [n_states][n_rows]. */
+int tbpm_random_states(tbpm_ctx* ctx, int64_t n_rows, int seed, int first_sample,
+                       int n_states, int rank, int n_ran_samples, int state_kind,
+                       double* wf);
+
+/* Chebyshev coefficients of the Fermi (one_minus_fermi = 0) or 1 - Fermi
+ * operator (funcs.f90:60-123 get_Fermi_cheb_coef); coef holds nr_fermi
+ * doubles; returns n_cheb through *n_cheb. */
+int tbpm_fermi_cheb_coef(int nr_fermi, double beta, double mu, int one_minus_fermi,
+                         double eps, double* coef, int* n_cheb);
+
+/* One time step psi <- exp(-/+ i H dt) psi of n_states states with the uploaded
+ * Hamiltonian (propagation.f90:12-49 cheb_wf_timestep).
+ * wf: complex128 [n_states][n_rows], in place. */
+int tbpm_cheb_timestep(tbpm_ctx* ctx, const double* bes, int n_bes, double* wf,
+                       int n_states, int forward);
+
+/* Fermi operator f(H) psi of n_states states with the uploaded Hamiltonian
+ * (propagation.f90:52-82 Fermi).  wf: complex128 [n_states][n_rows], in place. */
+int tbpm_fermi_apply(tbpm_ctx* ctx, const double* coef, int n_coef, double* wf,
+                     int n_states);
+
+/* ---- device-resident propagation session (benchmarks, batching) --------- */
+
+/* Start a DOS propagation of n_states random states (seed rule as
+ * tbpm_random_states with first_sample = 1) on the uploaded Hamiltonian, with
+ * room for n_timestep steps.  Records corr(0). */
+int tbpm_session_dos_begin(tbpm_ctx* ctx, const double* bes, int n_bes, int n_states,
+                           int seed, int rank, int n_ran_samples, int n_timestep);
+/* Enqueue n_steps time steps on the context stream; returns without waiting. */
+int tbpm_session_advance(tbpm_ctx* ctx, int n_steps);
+/* Wait for the stream and copy the per-state correlations recorded so far:
+ * corr complex128 [n_rows_done][n_states], norms float64 [n_rows_done][n_states]
+ * (either may be NULL).  *n_done receives the number of recorded time rows. */
+int tbpm_session_read(tbpm_ctx* ctx, double* corr, double* norms, int* n_done);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TBPM_B200_H */

@@ -1,0 +1,76 @@
+// Shared device-side types for the TBPM kernels (sm_100a).
+//
+// State vectors are stored "row-interleaved": a block of B states over N
+// orbitals is one array of N rows x ld complex numbers (ld = B, or 3B / 2B when
+// several vector families are propagated together), so the gather of
+// neighbour row c in the SpMV reads ld*sizeof(complex) contiguous bytes.
+// Each thread owns V consecutive complex columns of a row, loaded as one 16-byte
+// vector (double2 for FP64, float4 for FP32 pairs) or one 8-byte float2.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tbpm {
+
+template <typename R>
+struct Cx;
+template <>
+struct Cx<double> {
+  using t = double2;
+};
+template <>
+struct Cx<float> {
+  using t = float2;
+};
+
+// V complex numbers of precision R moved as one vector access.
+template <typename R, int V>
+struct alignas(2 * V * sizeof(R)) Pack {
+  R v[2 * V];
+};
+
+__device__ __forceinline__ Pack<double, 1> ldg_pack(const Pack<double, 1>* p) {
+  const double2 d = __ldg(reinterpret_cast<const double2*>(p));
+  Pack<double, 1> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  return r;
+}
+__device__ __forceinline__ Pack<float, 2> ldg_pack(const Pack<float, 2>* p) {
+  const float4 d = __ldg(reinterpret_cast<const float4*>(p));
+  Pack<float, 2> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  r.v[2] = d.z;
+  r.v[3] = d.w;
+  return r;
+}
+__device__ __forceinline__ Pack<float, 1> ldg_pack(const Pack<float, 1>* p) {
+  const float2 d = __ldg(reinterpret_cast<const float2*>(p));
+  Pack<float, 1> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  return r;
+}
+
+__device__ __forceinline__ double2 ldg_c(const double2* p) { return __ldg(p); }
+__device__ __forceinline__ float2 ldg_c(const float2* p) { return __ldg(p); }
+
+// Fixed-order tree reduction over the `rows` row slots of a block.  Values are
+// laid out as smem[slot * width + k]; after the call slot 0 holds the sums.
+// Every thread of the block must call it (it synchronises).
+__device__ __forceinline__ void tree_reduce_slots(double* smem, int rows, int width, int slot,
+                                                  int lane_lo, int lane_step) {
+  int s = 1;
+  while (s * 2 < rows) s *= 2;
+  for (; s > 0; s >>= 1) {
+    if (slot < s && slot + s < rows) {
+      for (int k = lane_lo; k < width; k += lane_step)
+        smem[slot * width + k] += smem[(slot + s) * width + k];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace tbpm

@@ -1,0 +1,1303 @@
+// Engine of libtbpm_b200: buffers, launch plans, CUDA-graph replay and the
+// drivers behind the C ABI.  The numerics live in tbpm_kernels.cuh.
+//
+// Data layout in HBM (one context):
+//   Hamiltonian  indptr int32[N+1], indices int32[nnz], hop complex[nnz] in the
+//                context precision (+ dx, dy real[nnz] for the current operator)
+//   A            the state block being propagated, row-interleaved [N][ld]
+//   X, Y         the two Chebyshev work vectors p_{k-1}, p_{k-2}  [N][ld]
+//   wf0          the initial states (correlation reference)       [N][B]
+//   partials     block partial sums of the fused reductions
+//   out          per-step reduced values [rows][ld][nv] (FP64)
+//   ctr          device step counter + finalize completion counter
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <type_traits>
+
+#include "tbpm_engine.cuh"
+#include "tbpm_dc_kernels.cuh"
+#include "tbpm_kernels.cuh"
+
+namespace tbpm {
+
+void throw_cuda(cudaError_t e, const char* what) {
+  (void)cudaGetLastError();  // clear sticky-free errors
+  const int code = e == cudaErrorMemoryAllocation ? TBPM_ERR_OOM : TBPM_ERR_CUDA;
+  throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+void DevMem::ensure(size_t n) {
+  if (n <= bytes && p) return;
+  release();
+  if (n == 0) n = 16;
+  TBPM_CK(cudaMalloc(&p, n));
+  bytes = n;
+}
+
+void DevMem::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+void GraphCache::reset() {
+  if (exec) cudaGraphExecDestroy(exec);
+  exec = nullptr;
+  key.clear();
+  steps = 0;
+}
+
+Expansion time_step_expansion(const double* bes, int n_bes) {
+  // propagation.f90:33-48 with img_dt = +i (forward); backward columns are
+  // selected through neg_mask (alpha -> -alpha).
+  Expansion e;
+  e.n_terms = n_bes;
+  e.alpha1_re = 0.0;
+  e.alpha1_im = -1.0;
+  e.alpha_re = 0.0;
+  e.alpha_im = -2.0;
+  e.beta = 1.0;
+  for (int s = 0; s < 2; ++s) {
+    e.w[s].resize(n_bes);
+    e.w[s][0] = bes[0];
+    for (int k = 1; k < n_bes; ++k) e.w[s][k] = 2 * bes[k];
+  }
+  return e;
+}
+
+Expansion fermi_expansion(const double* coef_a, int n_a, const double* coef_b, int n_b,
+                          unsigned long long set_b_mask) {
+  // propagation.f90:66-81: T0 = H psi, T1 = 2 H T0 - psi, p2 = 2 H p1 - p0.
+  Expansion e;
+  e.n_terms = std::max(n_a, n_b);
+  e.alpha1_re = 1.0;
+  e.alpha1_im = 0.0;
+  e.alpha_re = 2.0;
+  e.alpha_im = 0.0;
+  e.beta = -1.0;
+  e.w[0].assign(e.n_terms, 0.0);
+  e.w[1].assign(e.n_terms, 0.0);
+  for (int k = 0; k < n_a; ++k) e.w[0][k] = coef_a[k];
+  for (int k = 0; k < n_b; ++k) e.w[1][k] = coef_b[k];
+  e.set_mask = set_b_mask;
+  return e;
+}
+
+namespace {
+
+constexpr int kSMs = 148;
+
+template <typename R, int V_>
+struct Prec {
+  using Real = R;
+  static constexpr int V = V_;
+};
+
+template <class F>
+void dispatch(int prec, int V, F&& f) {
+  if (prec == TBPM_PREC_FP64)
+    f(Prec<double, 1>{});
+  else if (V == 2)
+    f(Prec<float, 2>{});
+  else
+    f(Prec<float, 1>{});
+}
+
+inline size_t real_size(int prec) { return prec == TBPM_PREC_FP64 ? 8 : 4; }
+
+Tile pick_tile(const tbpm_ctx* c, int64_t n_rows, int tpr) {
+  Tile t;
+  int want = c->opts.threads_per_block > 0 ? c->opts.threads_per_block : 256;
+  want = std::min(std::max(want, 32), 512);
+  t.rpp = std::max(1, want / tpr);
+  while (t.rpp * tpr > 512 && t.rpp > 1) --t.rpp;
+  t.threads = t.rpp * tpr;
+  int64_t passes;
+  if (c->opts.rows_per_tile > 0) {
+    passes = std::max<int64_t>(1, c->opts.rows_per_tile / t.rpp);
+  } else {
+    // aim at >= 16 resident-block waves of work while keeping the partial
+    // sums small
+    const int64_t target_blocks = (int64_t)kSMs * 16;
+    passes = n_rows / ((int64_t)t.rpp * target_blocks);
+    passes = std::min<int64_t>(std::max<int64_t>(passes, 1), 64);
+  }
+  t.rows_per_tile = (int64_t)t.rpp * passes;
+  t.grid = (int)((n_rows + t.rows_per_tile - 1) / t.rows_per_tile);
+  if (t.grid < 1) t.grid = 1;
+  return t;
+}
+
+// ---- small utility kernels -------------------------------------------------
+
+// dst[r*ld + col0 + s] = src[s*n + r]   (host C-order states -> interleaved)
+template <typename R>
+__global__ void interleave_kernel(const double2* src, int ns, int64_t n, int ld, int col0,
+                                  typename Cx<R>::t* dst) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n * ns) return;
+  const int64_t r = gid / ns;
+  const int s = (int)(gid - r * ns);
+  const double2 v = src[(int64_t)s * n + r];
+  typename Cx<R>::t o;
+  o.x = (R)v.x;
+  o.y = (R)v.y;
+  dst[r * ld + col0 + s] = o;
+}
+
+// dst[s*n + r] = src[r*ld + col0 + s]   (interleaved -> host C-order states)
+template <typename R>
+__global__ void deinterleave_kernel(const typename Cx<R>::t* src, int ns, int64_t n, int ld,
+                                    int col0, double2* dst) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= n * ns) return;
+  const int s = (int)(gid / n);
+  const int64_t r = gid - (int64_t)s * n;
+  const typename Cx<R>::t v = src[r * ld + col0 + s];
+  dst[gid] = make_double2((double)v.x, (double)v.y);
+}
+
+__global__ void cast_f64_to_f32_kernel(const double* src, int64_t n, float* dst) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid < n) dst[gid] = (float)src[gid];
+}
+
+inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
+
+// ---- launch helpers ----------------------------------------------------------
+
+struct Counters {
+  int* step;
+  unsigned int* done;
+};
+
+Counters counters(tbpm_ctx* c, int which) {
+  int* base = c->ctr.as<int>();
+  return Counters{base + 2 * which, reinterpret_cast<unsigned int*>(base + 2 * which + 1)};
+}
+
+void reset_counters(tbpm_ctx* c, int which) {
+  TBPM_CK(cudaMemsetAsync(c->ctr.as<int>() + 2 * which, 0, 2 * sizeof(int), c->stream));
+}
+
+void launch_finalize(tbpm_ctx* c, int grid_parts, int n_values, Counters k, double* out) {
+  finalize_kernel<<<n_values, 256, 0, c->stream>>>(c->partials.as<double>(), grid_parts, n_values,
+                                                    k.step, k.done, out);
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+}
+
+void ensure_partials(tbpm_ctx* c, size_t n_doubles) {
+  c->partials.ensure(std::max<size_t>(n_doubles, 64) * sizeof(double));
+}
+
+template <typename R, int V>
+void launch_term(tbpm_ctx* c, const Tile& t, const TermArgs<R, V>& a) {
+  const size_t smem = a.partials ? (size_t)t.threads * V * 3 * sizeof(double) : 0;
+  cheb_term_kernel<R, V><<<t.grid, t.threads, smem, c->stream>>>(a);
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+}
+
+// Enqueue one expansion (one time step, or one Fermi operator) on the block A.
+// When `partials_out` is set the last term also produces <ref|psi>, <psi|psi>
+// block partials and a finalize launch stores them in out[*step].
+template <typename R, int V>
+void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, Pack<R, V>* X,
+                       Pack<R, V>* Y, const Pack<R, V>* ref, int ref_ld, double* partials_out,
+                       Counters k_ctr, Pack<R, V>* A_out = nullptr) {
+  // A holds psi (p_0) on entry; the expansion result goes to A_out (default A).
+  if (!A_out) A_out = A;
+  const Ham& h = c->ham;
+  const int tpr = ld / V;
+  const Tile t = pick_tile(c, h.n, tpr);
+  const bool want = partials_out != nullptr;
+  if (want) ensure_partials(c, (size_t)ld * 3 * t.grid);
+  auto buf = [&](int k) { return (k & 1) ? X : Y; };
+  const int n = ex.n_terms;
+  int last_flush = -1;
+  const size_t sv = 2 * sizeof(R);
+  const double vec = (double)h.n * ld * sv;
+  const double mat = (double)(h.n + 1) * 4 + (double)h.nnz * (4 + 2 * sizeof(R));
+  for (int k = 1; k < n; ++k) {
+    TermArgs<R, V> a{};
+    a.indptr = h.indptr.as<int32_t>();
+    a.indices = h.indices.as<int32_t>();
+    a.hop = h.hop.as<typename Cx<R>::t>();
+    a.n_rows = h.n;
+    a.rows_per_tile = t.rows_per_tile;
+    a.tpr = tpr;
+    a.c.neg_mask = ex.neg_mask;
+    a.c.set_mask = ex.set_mask;
+    double bytes = mat + vec;  // gather of p_{k-1}
+    if (k == 1) {
+      a.c.alpha_re = ex.alpha1_re;
+      a.c.alpha_im = ex.alpha1_im;
+      a.c.beta = 0.0;
+      a.gather = A;
+      a.pin = nullptr;
+      a.pout = X;
+      a.c.nflush = 0;
+      bytes += vec;
+    } else {
+      a.c.alpha_re = ex.alpha_re;
+      a.c.alpha_im = ex.alpha_im;
+      a.c.beta = ex.beta;
+      a.gather = buf(k - 1);
+      a.pin = (k == 2) ? A : buf(k);
+      a.pout = (k < n - 1) ? buf(k) : nullptr;
+      bytes += vec * (a.pout ? 2 : 1);
+      const int pending = k - last_flush;
+      const bool flush = (k == 2) || pending == 3 || k == n - 1;
+      if (flush) {
+        a.c.nflush = pending;
+        a.c.acc_init = (k == 2) ? 1 : 0;
+        for (int s = 0; s < 2; ++s) {
+          a.c.w[s][0] = pending >= 3 ? ex.w[s][k - 2] : 0.0;
+          a.c.w[s][1] = pending >= 2 ? ex.w[s][k - 1] : 0.0;
+          a.c.w[s][2] = ex.w[s][k];
+        }
+        a.acc = A_out;
+        last_flush = k;
+        bytes += vec * (a.c.acc_init ? 1 : 2);
+      }
+    }
+    if (k == n - 1 && want) {
+      a.ref = ref;
+      a.ref_tpr = ref ? ref_ld / V : 0;
+      a.partials = c->partials.as<double>();
+      if (ref) bytes += (double)h.n * ref_ld * sv;
+    }
+    launch_term<R, V>(c, t, a);
+    c->model_bytes += bytes;
+  }
+  if (want) launch_finalize(c, t.grid, ld * 3, k_ctr, partials_out);
+}
+
+template <typename R, int V>
+void enqueue_corr(tbpm_ctx* c, const Pack<R, V>* x, const Pack<R, V>* ref, int ld, int ref_ld,
+                  double* out, Counters k_ctr) {
+  const int tpr = ld / V;
+  const Tile t = pick_tile(c, c->ham.n, tpr);
+  ensure_partials(c, (size_t)ld * 3 * t.grid);
+  const size_t smem = (size_t)t.threads * V * 3 * sizeof(double);
+  corr_kernel<R, V><<<t.grid, t.threads, smem, c->stream>>>(
+      x, ref, c->ham.n, t.rows_per_tile, tpr, ref ? ref_ld / V : 0, c->partials.as<double>());
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  launch_finalize(c, t.grid, ld * 3, k_ctr, out);
+}
+
+// Random states of the reference distribution into dst (row-interleaved, ld
+// columns starting at column 0).  keys[col] = iseed * 49741.
+template <typename R, int V>
+void gen_states(tbpm_ctx* c, const StateKeys& keys, int ld, int kind, Pack<R, V>* dst) {
+  const int tpr = ld / V;
+  const Tile t = pick_tile(c, c->ham.n, tpr);
+  ensure_partials(c, (size_t)ld * t.grid);
+  c->small.ensure(sizeof(double) * kMaxCols * 2);
+  reset_counters(c, 1);
+  const size_t smem = (size_t)t.threads * V * sizeof(double);
+  gen_state_kernel<R, V><<<t.grid, t.threads, smem, c->stream>>>(
+      keys, kind, c->ham.n, t.rows_per_tile, tpr, 0, nullptr, 1, dst, c->partials.as<double>());
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  launch_finalize(c, t.grid, ld, counters(c, 1), c->small.as<double>());
+  gen_state_kernel<R, V><<<t.grid, t.threads, 0, c->stream>>>(
+      keys, kind, c->ham.n, t.rows_per_tile, tpr, 1, c->small.as<double>(), 1, dst, nullptr);
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+}
+
+// Host states (complex128 [ns][n]) -> columns [col0, col0+ns) of dst.
+template <typename R>
+void upload_states(tbpm_ctx* c, const double* host, int ns, int ld, int col0, void* dst) {
+  const int64_t n = c->ham.n;
+  const size_t bytes = (size_t)n * ns * 16;
+  c->stage.ensure(bytes);
+  TBPM_CK(cudaMemcpyAsync(c->stage.p, host, bytes, cudaMemcpyHostToDevice, c->stream));
+  interleave_kernel<R><<<blocks_for(n * ns, 256), 256, 0, c->stream>>>(
+      c->stage.as<double2>(), ns, n, ld, col0, reinterpret_cast<typename Cx<R>::t*>(dst));
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+}
+
+// Columns [col0, col0+ns) of src -> host complex128 [ns][n] (synchronous).
+template <typename R>
+void download_states(tbpm_ctx* c, const void* src, int ns, int ld, int col0, double* host) {
+  const int64_t n = c->ham.n;
+  const size_t bytes = (size_t)n * ns * 16;
+  c->stage.ensure(bytes);
+  deinterleave_kernel<R><<<blocks_for(n * ns, 256), 256, 0, c->stream>>>(
+      reinterpret_cast<const typename Cx<R>::t*>(src), ns, n, ld, col0, c->stage.as<double2>());
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  TBPM_CK(cudaMemcpyAsync(host, c->stage.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+}
+
+void ensure_vectors(tbpm_ctx* c, int ld, int ref_ld) {
+  const size_t vb = (size_t)c->ham.n * ld * 2 * real_size(c->ham.prec);
+  c->A.ensure(vb);
+  c->X.ensure(vb);
+  c->Y.ensure(vb);
+  c->wf0.ensure((size_t)c->ham.n * std::max(ref_ld, 1) * 2 * real_size(c->ham.prec));
+  c->ctr.ensure(16 * sizeof(int));
+}
+
+StateKeys make_keys(int seed, int first_sample, int n_states, int rank, int n_ran_samples) {
+  // tbpm.f90:57 iseed = seed*(i_sample + rank*n_ran_samples); random.f90:52
+  // iseed0 = iseed*49741 seeds the stream.
+  StateKeys k{};
+  for (int i = 0; i < n_states && i < kMaxCols; ++i) {
+    const long long iseed = (long long)seed * ((long long)first_sample + i +
+                                               (long long)rank * n_ran_samples);
+    k.key[i] = iseed * 49741LL;
+  }
+  return k;
+}
+
+int pick_V(int prec, int ld, int group) {
+  if (prec == TBPM_PREC_FP64) return 1;
+  return (ld % 2 == 0 && group % 2 == 0) ? 2 : 1;
+}
+
+void require_ham(const tbpm_ctx* c, bool need_dxy) {
+  if (c->ham.n <= 0) throw Error{TBPM_ERR_STATE, "no Hamiltonian uploaded"};
+  if (c->ham.prec != c->opts.precision)
+    throw Error{TBPM_ERR_STATE,
+                "the uploaded Hamiltonian has a different precision than the context options; "
+                "upload it again"};
+  if (need_dxy && !c->ham.has_dxy)
+    throw Error{TBPM_ERR_ARG, "dx/dy are required (current operator) but were not uploaded"};
+}
+
+int batch_size(const tbpm_ctx* c) {
+  int b = c->opts.batch > 0 ? c->opts.batch : 16;
+  return std::min(b, kMaxCols);
+}
+
+// ---- CUDA graph replay of a per-step program ---------------------------------
+
+template <class Fn>
+void run_steps(tbpm_ctx* c, int n_steps, const std::vector<unsigned char>& key, Fn&& step) {
+  if (n_steps <= 0) return;
+  const int G = c->opts.steps_per_graph > 0 ? c->opts.steps_per_graph : 16;
+  int done = 0;
+  if (c->opts.use_graphs && n_steps >= G) {
+    if (!c->graph.exec || c->graph.key != key || c->graph.steps != G) {
+      c->graph.reset();
+      const int64_t l0 = c->launches;
+      const double b0 = c->model_bytes;
+      TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+      try {
+        for (int i = 0; i < G; ++i) step();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      cudaGraph_t g = nullptr;
+      TBPM_CK(cudaStreamEndCapture(c->stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&c->graph.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        c->graph.exec = nullptr;
+        throw_cuda(e, "cudaGraphInstantiate");
+      }
+      c->graph.key = key;
+      c->graph.steps = G;
+      // capture does not execute: undo the counters recorded during capture
+      c->launches = l0;
+      c->model_bytes = b0;
+      // measure launches/bytes of one step by enqueuing nothing: recompute
+      // below from a dry count
+    }
+    // per-step launch/byte counts are identical for every replayed step
+    int64_t l_step = 0;
+    double b_step = 0;
+    {
+      const int64_t l0 = c->launches;
+      const double b0 = c->model_bytes;
+      // counting pass: run the plan builder under capture into a throwaway graph
+      TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+      try {
+        step();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      cudaGraph_t g = nullptr;
+      TBPM_CK(cudaStreamEndCapture(c->stream, &g));
+      if (g) cudaGraphDestroy(g);
+      l_step = c->launches - l0;
+      b_step = c->model_bytes - b0;
+      c->launches = l0;
+      c->model_bytes = b0;
+    }
+    while (n_steps - done >= G) {
+      TBPM_CK(cudaGraphLaunch(c->graph.exec, c->stream));
+      c->launches += l_step * G;
+      c->model_bytes += b_step * G;
+      done += G;
+    }
+  }
+  for (; done < n_steps; ++done) step();
+}
+
+template <typename T>
+void key_push(std::vector<unsigned char>& k, const T& v) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), p, p + sizeof(T));
+}
+
+std::vector<unsigned char> plan_key(const tbpm_ctx* c, int kind, int ld, int V,
+                                    const Expansion& ex) {
+  std::vector<unsigned char> k;
+  key_push(k, kind);
+  key_push(k, ld);
+  key_push(k, V);
+  key_push(k, c->ham.prec);
+  key_push(k, c->ham.n);
+  key_push(k, c->ham.nnz);
+  const void* ptrs[] = {c->ham.indptr.p, c->ham.indices.p, c->ham.hop.p, c->ham.dx.p,
+                        c->ham.dy.p,     c->A.p,           c->X.p,       c->Y.p,
+                        c->wf0.p,        c->partials.p,    c->out.p,     c->ctr.p};
+  for (const void* p : ptrs) key_push(k, p);
+  key_push(k, c->opts.threads_per_block);
+  key_push(k, c->opts.rows_per_tile);
+  key_push(k, ex.n_terms);
+  key_push(k, ex.neg_mask);
+  key_push(k, ex.set_mask);
+  for (int s = 0; s < 2; ++s)
+    for (double w : ex.w[s]) key_push(k, w);
+  return k;
+}
+
+// ---- norm check (funcs.f90:175-192) -----------------------------------------
+
+double effective_thr(const tbpm_ctx* c, double thr) {
+  if (c->ham.prec == TBPM_PREC_FP32) return std::max(thr, c->opts.fp32_chk_thr);
+  return thr;
+}
+
+bool norm_broken(double norm, double ref, double thr) {
+  const double d = std::fabs(norm - ref);
+  return std::isnan(d) || !std::isfinite(d) || d > thr;
+}
+
+void raise_norm(const char* where, int t) {
+  char buf[320];
+  std::snprintf(buf, sizeof buf,
+                "%s: wave function norm gets broken during propagation (time step %d). "
+                "Check the Hermitianity of the Hamiltonian, then try increasing 'rescale'.",
+                where, t);
+  throw Error{TBPM_ERR_NORM, buf};
+}
+
+void read_out(tbpm_ctx* c, std::vector<double>& host, size_t n_doubles) {
+  host.resize(n_doubles);
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  if (n_doubles)
+    TBPM_CK(cudaMemcpy(host.data(), c->out.p, n_doubles * sizeof(double), cudaMemcpyDeviceToHost));
+}
+
+// ---- DOS ----------------------------------------------------------------------
+
+template <typename R, int V>
+void dos_session_begin(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys* keys,
+                       const double* host_wf0, int rows_cap) {
+  c->graph.reset();
+  ensure_vectors(c, ns, ns);
+  c->out.ensure((size_t)rows_cap * ns * 3 * sizeof(double));
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  if (keys)
+    gen_states<R, V>(c, *keys, ns, c->opts.state_kind, W);
+  else
+    upload_states<R>(c, host_wf0, ns, ns, 0, W);
+  TBPM_CK(cudaMemcpyAsync(A, W, (size_t)c->ham.n * ns * 2 * sizeof(R), cudaMemcpyDeviceToDevice,
+                          c->stream));
+  reset_counters(c, 0);
+  enqueue_corr<R, V>(c, A, W, ns, ns, c->out.as<double>(), counters(c, 0));
+  c->sess.active = true;
+  c->sess.kind = 1;
+  c->sess.ld = ns;
+  c->sess.V = V;
+  c->sess.rows_cap = rows_cap;
+  c->sess.rows_enqueued = 1;
+  c->sess.ex = ex;
+}
+
+template <typename R, int V>
+void dos_session_advance(tbpm_ctx* c, int n_steps) {
+  Session& s = c->sess;
+  if (!s.active || s.kind != 1) throw Error{TBPM_ERR_STATE, "no DOS session active"};
+  if (s.rows_enqueued + n_steps > s.rows_cap)
+    throw Error{TBPM_ERR_ARG, "session capacity (n_timestep) exceeded"};
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  const int ld = s.ld;
+  const Expansion& ex = s.ex;
+  auto step = [&]() {
+    enqueue_expansion<R, V>(c, ex, ld, A, X, Y, W, ld, c->out.as<double>(), counters(c, 0));
+  };
+  run_steps(c, n_steps, plan_key(c, 1, ld, V, ex), step);
+  s.rows_enqueued += n_steps;
+}
+
+// Run one batch of DOS states and accumulate into corr (complex, n_t+1),
+// optionally storing per-state correlations.
+template <typename R, int V>
+void dos_batch(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys* keys,
+               const double* host_wf0, int n_timestep, int chk_step, double chk_thr,
+               int n_avg, double* corr, double* corr_per_state, int state_offset,
+               int total_states) {
+  dos_session_begin<R, V>(c, ex, ns, keys, host_wf0, n_timestep + 1);
+  const double thr = effective_thr(c, chk_thr);
+  std::vector<double> host;
+  // tbpm.f90:71-79: the norm of wf_t(t-1) is checked at t == chk_step against
+  // norm_ref = <wf_1|wf_1>; rows hold the state after `row` steps.
+  const bool check = chk_step >= 2 && chk_step <= n_timestep;
+  int done = 0;
+  if (check) {
+    dos_session_advance<R, V>(c, chk_step - 1);
+    done = chk_step - 1;
+    read_out(c, host, (size_t)(done + 1) * ns * 3);
+    for (int b = 0; b < ns; ++b) {
+      const double ref = host[((size_t)1 * ns + b) * 3 + 2];
+      const double nv = host[((size_t)(chk_step - 1) * ns + b) * 3 + 2];
+      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dos", chk_step);
+    }
+  }
+  dos_session_advance<R, V>(c, n_timestep - done);
+  read_out(c, host, (size_t)(n_timestep + 1) * ns * 3);
+  c->sess.active = false;
+  // tbpm.f90:58-86: corr(t) += corrval / n_ran_samples, sample by sample
+  for (int b = 0; b < ns; ++b) {
+    for (int t = 0; t <= n_timestep; ++t) {
+      const double re = host[((size_t)t * ns + b) * 3 + 0];
+      const double im = host[((size_t)t * ns + b) * 3 + 1];
+      corr[2 * t] += re / n_avg;
+      corr[2 * t + 1] += im / n_avg;
+      if (corr_per_state) {
+        double* o = corr_per_state + 2 * ((size_t)(state_offset + b) * (n_timestep + 1) + t);
+        o[0] = re;
+        o[1] = im;
+      }
+    }
+  }
+  (void)total_states;
+}
+
+// ---- AC ---------------------------------------------------------------------
+
+template <typename R, int V>
+void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, int nb,
+              const StateKeys* keys, const double* host_wf0, int n_timestep, int chk_step,
+              double chk_thr, int n_avg, double* corr) {
+  const int ld = 3 * nb;
+  c->graph.reset();
+  ensure_vectors(c, ld, nb);
+  c->out.ensure((size_t)std::max(n_timestep, 1) * nb * 9 * sizeof(double));
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  const Ham& h = c->ham;
+  if (keys)
+    gen_states<R, V>(c, *keys, nb, c->opts.state_kind, W);
+  else
+    upload_states<R>(c, host_wf0, nb, nb, 0, W);
+  // [J_x wf0 | J_y wf0 | wf0] (tbpm.f90:277-278)
+  current_apply_kernel<R><<<blocks_for(h.n * nb, 256), 256, 0, c->stream>>>(
+      h.indptr.as<int32_t>(), h.indices.as<int32_t>(), h.hop.as<typename Cx<R>::t>(),
+      h.dx.as<R>(), h.dy.as<R>(), h.rescale, h.n, nb,
+      reinterpret_cast<const typename Cx<R>::t*>(W), reinterpret_cast<typename Cx<R>::t*>(A));
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  // Fermi operators (tbpm.f90:279-281): 1-F on the current columns, F on wf0
+  enqueue_expansion<R, V>(c, ex_fermi, ld, A, X, Y, nullptr, 0, nullptr, Counters{});
+  const Tile tj = pick_tile(c, h.n, nb);
+  const size_t smem_j = (size_t)tj.threads * 9 * sizeof(double);
+  reset_counters(c, 0);
+  auto jcorr = [&]() {
+    ensure_partials(c, (size_t)nb * 9 * tj.grid);
+    jcorr_kernel<R><<<tj.grid, tj.threads, smem_j, c->stream>>>(
+        h.indptr.as<int32_t>(), h.indices.as<int32_t>(), h.hop.as<typename Cx<R>::t>(),
+        h.dx.as<R>(), h.dy.as<R>(), h.rescale, h.n, tj.rows_per_tile, nb,
+        reinterpret_cast<const typename Cx<R>::t*>(A), c->partials.as<double>());
+    TBPM_CK(cudaGetLastError());
+    c->launches++;
+    c->model_bytes += (double)(h.n + 1) * 4 + (double)h.nnz * (4 + 4 * sizeof(R)) +
+                      (double)h.n * nb * 3 * 2 * sizeof(R);
+    launch_finalize(c, tj.grid, nb * 9, counters(c, 0), c->out.as<double>());
+  };
+  // row 0: after the Fermi operators (t = 1, not accumulated; its psi2 norm is
+  // the norm reference of tbpm.f90:307)
+  jcorr();
+  auto step = [&]() {
+    enqueue_expansion<R, V>(c, ex_time, ld, A, X, Y, nullptr, 0, nullptr, Counters{});
+    jcorr();
+  };
+  const double thr = effective_thr(c, chk_thr);
+  std::vector<double> host;
+  int done = 0;  // propagation steps enqueued; row r = after r steps
+  const bool check = chk_step >= 2 && chk_step <= n_timestep;
+  const auto key = plan_key(c, 2, ld, V, ex_time);
+  if (check) {
+    // at t == chk_step psi2 has been propagated chk_step-2 times
+    run_steps(c, chk_step - 2, key, step);
+    done = chk_step - 2;
+    read_out(c, host, (size_t)(done + 1) * nb * 9);
+    for (int b = 0; b < nb; ++b) {
+      const double ref = host[(size_t)b * 9 + 8];
+      const double nv = host[((size_t)done * nb + b) * 9 + 8];
+      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_accond", chk_step);
+    }
+  }
+  run_steps(c, (n_timestep - 1) - done, key, step);
+  const int rows = std::max(n_timestep, 1);
+  read_out(c, host, (size_t)rows * nb * 9);
+  // corr(k, t) for t = 2..n_timestep is row t-1 (tbpm.f90:346-349)
+  for (int b = 0; b < nb; ++b)
+    for (int t = 2; t <= n_timestep; ++t)
+      for (int k = 0; k < 4; ++k) {
+        const double re = host[((size_t)(t - 1) * nb + b) * 9 + 2 * k];
+        const double im = host[((size_t)(t - 1) * nb + b) * 9 + 2 * k + 1];
+        corr[2 * (k + 4 * (size_t)(t - 1))] += re / n_avg;
+        corr[2 * (k + 4 * (size_t)(t - 1)) + 1] += im / n_avg;
+      }
+}
+
+
+// ---- DC -----------------------------------------------------------------------
+
+// One batch of nb states of tbpm_dccond (tbpm.f90:586-698).
+template <typename R, int V>
+void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int nb,
+              const StateKeys* keys, const double* host_wf0, int n_timestep, double t_step,
+              const std::vector<double>& en_sel, int chk_step, double chk_thr, int n_avg,
+              int n_energies, double* dos_corr, double* dc_corr) {
+  using C = typename Cx<R>::t;
+  const Ham& h = c->ham;
+  const int64_t n = h.n;
+  const int ld = 2 * nb;
+  const int n_en = (int)en_sel.size();
+  const int T1 = std::min(kMaxWindow, std::max(n_timestep, 1));  // phase-1 window
+  const int T2 = std::min(8, std::max(n_timestep, 1));           // phase-2 window
+  const size_t vb = (size_t)n * ld * 2 * sizeof(R);
+  c->graph.reset();
+  c->X.ensure(vb);
+  c->Y.ensure(vb);
+  c->A.ensure(vb * (size_t)(std::max(T1, T2) + 1));
+  c->wf0.ensure((size_t)n * nb * 2 * sizeof(R));
+  c->ctr.ensure(16 * sizeof(int));
+  c->out.ensure((size_t)std::max(n_timestep, 1) * ld * 3 * sizeof(double));
+  c->small.ensure(sizeof(double) * 3 * kMaxCols * 2);
+  const size_t qe_bytes = (size_t)n * std::max(n_en, 1) * nb * 2 * sizeof(R);
+  c->qe.ensure(qe_bytes);
+  c->coef.ensure(sizeof(double2) * (size_t)kMaxWindow * std::max(n_en, 1));
+  auto slot = [&](int s) { return reinterpret_cast<Pack<R, V>*>(c->A.as<char>() + vb * s); };
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  C* qe = c->qe.as<C>();
+  if (keys)
+    gen_states<R, V>(c, *keys, nb, c->opts.state_kind, W);
+  else
+    upload_states<R>(c, host_wf0, nb, nb, 0, W);
+  // wf_t_pos = wf_t_neg = wf0 in the slot read by the first step
+  dup_columns_kernel<R><<<blocks_for(n * nb, 256), 256, 0, c->stream>>>(
+      reinterpret_cast<const C*>(W), n, nb, reinterpret_cast<C*>(slot(T1 - 1)));
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  // norm_ref = <wf0|wf0> (tbpm.f90:606) for every column
+  reset_counters(c, 2);
+  enqueue_corr<R, V>(c, slot(T1 - 1), nullptr, ld, 0, c->small.as<double>(), counters(c, 2));
+  std::vector<double> norm_ref(3 * ld);
+  TBPM_CK(cudaMemcpyAsync(norm_ref.data(), c->small.p, norm_ref.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  const double thr = effective_thr(c, chk_thr);
+  reset_counters(c, 0);
+  const bool check = chk_step >= 2 && chk_step <= n_timestep;
+  std::vector<double2> coef_host((size_t)kMaxWindow * std::max(n_en, 1));
+  std::vector<double> host;
+  const double pi = 3.14159265358979323846;
+  // ---- phase 1: +/- dt propagation, DOS correlation, QE accumulation ----
+  int t = 1;
+  bool first_window = true;
+  while (t <= n_timestep) {
+    int len = std::min(T1, n_timestep - t + 1);
+    if (check && t <= chk_step - 1 && t + len - 1 > chk_step - 1) len = chk_step - t;
+    for (int tau = 0; tau < len; ++tau) {
+      Pack<R, V>* in = slot(tau == 0 ? T1 - 1 : tau - 1);
+      enqueue_expansion<R, V>(c, ex_pm, ld, in, X, Y, W, nb, c->out.as<double>(),
+                              counters(c, 0), slot(tau));
+    }
+    if (n_en > 0) {
+      for (int tau = 0; tau < len; ++tau) {
+        const int tt = t + tau;
+        const double Wh = 0.5 * (1 + std::cos(pi * tt / n_timestep));  // Hanning
+        for (int i = 0; i < n_en; ++i) {
+          const double x = en_sel[i] * (double)tt * t_step;
+          coef_host[(size_t)tau * n_en + i] = make_double2(Wh * std::cos(x), Wh * std::sin(x));
+        }
+      }
+      TBPM_CK(cudaMemcpyAsync(c->coef.p, coef_host.data(), sizeof(double2) * len * n_en,
+                              cudaMemcpyHostToDevice, c->stream));
+      StatePtrs<R> win{};
+      for (int tau = 0; tau < len; ++tau) win.p[tau] = reinterpret_cast<const C*>(slot(tau));
+      const int64_t total = n * n_en * nb;
+      const int grid = (int)std::min<int64_t>(blocks_for(total, 256), (int64_t)kSMs * 64);
+      qe_accum_kernel<R><<<grid, 256, 0, c->stream>>>(qe, n, n_en, nb, win, len,
+                                                        c->coef.as<double2>(),
+                                                        first_window ? 1 : 0,
+                                                        reinterpret_cast<const C*>(W));
+      TBPM_CK(cudaGetLastError());
+      c->launches++;
+      c->model_bytes += (double)total * 2 * sizeof(R) * (first_window ? 1 : 2) +
+                        (double)len * n * ld * 2 * sizeof(R);
+    }
+    // the window ring: the next window reads the last state from slot T1-1
+    if (len != T1 && t + len - 1 < n_timestep)
+      TBPM_CK(cudaMemcpyAsync(slot(T1 - 1), slot(len - 1), vb, cudaMemcpyDeviceToDevice,
+                              c->stream));
+    TBPM_CK(cudaStreamSynchronize(c->stream));  // coef_host is reused
+    first_window = false;
+    t += len;
+    if (check && t == chk_step) {
+      // tbpm.f90:611-614: at t == chk_step the states after chk_step-1 steps
+      read_out(c, host, (size_t)(chk_step - 1) * ld * 3);
+      for (int b = 0; b < ld; ++b) {
+        const double nv = host[((size_t)(chk_step - 2) * ld + b) * 3 + 2];
+        if (norm_broken(nv, norm_ref[(size_t)b * 3 + 2], thr)) raise_norm("tbpm_dccond", chk_step);
+      }
+    }
+  }
+  read_out(c, host, (size_t)n_timestep * ld * 3);
+  for (int b = 0; b < nb; ++b)
+    for (int tt = 1; tt <= n_timestep; ++tt) {
+      dos_corr[2 * (tt - 1)] += host[((size_t)(tt - 1) * ld + b) * 3 + 0] / n_avg;
+      dos_corr[2 * (tt - 1) + 1] += host[((size_t)(tt - 1) * ld + b) * 3 + 1] / n_avg;
+    }
+  if (n_en == 0) return;
+  // ---- phase 2 ----
+  const int n_ib = n_en * nb;
+  int64_t rows_per_tile = std::max<int64_t>(64, n / ((int64_t)kSMs * 8));
+  const int pgrid = (int)((n + rows_per_tile - 1) / rows_per_tile);
+  const int pthreads = std::min(256, ((n_ib + 31) / 32) * 32);
+  // |<wf0|QE_i>| per (energy, state)
+  ensure_partials(c, (size_t)2 * n_ib * pgrid);
+  c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
+  qe_project_kernel<R><<<pgrid, pthreads, 0, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
+                                                          StatePtrs<R>{}, 1, 1,
+                                                          reinterpret_cast<const C*>(W),
+                                                          c->partials.as<double>());
+  TBPM_CK(cudaGetLastError());
+  reduce_rows_kernel<<<(int)std::min<int64_t>(2 * n_ib, 65535), 256, 0, c->stream>>>(
+      c->partials.as<double>(), pgrid, 2 * n_ib, c->small.as<double>());
+  TBPM_CK(cudaGetLastError());
+  c->launches += 2;
+  std::vector<double> proj(2 * n_ib);
+  TBPM_CK(cudaMemcpyAsync(proj.data(), c->small.p, proj.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> amp(n_ib);
+  for (int ib = 0; ib < n_ib; ++ib) amp[ib] = std::hypot(proj[2 * ib], proj[2 * ib + 1]);
+  // wf0_J = [J_x wf0 | J_y wf0] (tbpm.f90:654-655) in slot T (the propagated block)
+  Pack<R, V>* wj = slot(std::max(T1, T2));
+  jj_apply_kernel<R><<<blocks_for(n * ld, 256), 256, 0, c->stream>>>(
+      h.indptr.as<int32_t>(), h.indices.as<int32_t>(), h.hop.as<C>(), h.dx.as<R>(), h.dy.as<R>(),
+      h.rescale, n, nb, reinterpret_cast<const C*>(W), nb, 0, 0, reinterpret_cast<C*>(wj));
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  ensure_partials(c, (size_t)2 * 2 * T2 * n_ib * pgrid);
+  std::vector<double> vals;
+  for (t = 1; t <= n_timestep; t += T2) {
+    const int len = std::min(T2, n_timestep - t + 1);
+    StatePtrs<R> u{};
+    for (int tau = 0; tau < len; ++tau) {
+      const int tt = t + tau;
+      if (tt >= 2)
+        enqueue_expansion<R, V>(c, ex_fwd, ld, wj, X, Y, nullptr, 0, nullptr, Counters{});
+      C* us = reinterpret_cast<C*>(slot(tau));
+      jj_apply_kernel<R><<<blocks_for(n * ld, 256), 256, 0, c->stream>>>(
+          h.indptr.as<int32_t>(), h.indices.as<int32_t>(), h.hop.as<C>(), h.dx.as<R>(),
+          h.dy.as<R>(), h.rescale, n, nb, reinterpret_cast<const C*>(wj), ld, 0, nb, us);
+      TBPM_CK(cudaGetLastError());
+      c->launches++;
+      u.p[tau] = us;
+    }
+    qe_project_kernel<R><<<pgrid, pthreads, 0, c->stream>>>(qe, n, rows_per_tile, n_en, nb, u,
+                                                            len, 0, nullptr,
+                                                            c->partials.as<double>());
+    TBPM_CK(cudaGetLastError());
+    const int64_t n_vals = (int64_t)2 * len * 2 * n_ib;
+    reduce_rows_kernel<<<(int)std::min<int64_t>(n_vals, 65535), 256, 0, c->stream>>>(
+        c->partials.as<double>(), pgrid, n_vals, c->small.as<double>());
+    TBPM_CK(cudaGetLastError());
+    c->launches += 2;
+    c->model_bytes += (double)n * n_ib * 2 * sizeof(R) + (double)len * n * ld * 2 * sizeof(R);
+    vals.resize(n_vals);
+    TBPM_CK(cudaMemcpyAsync(vals.data(), c->small.p, n_vals * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+    TBPM_CK(cudaStreamSynchronize(c->stream));
+    for (int tau = 0; tau < len; ++tau)
+      for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < n_en; ++i)
+          for (int b = 0; b < nb; ++b) {
+            const int ib = i * nb + b;
+            const int64_t o = ((int64_t)(tau * 2 + k) * n_ib + ib) * 2;
+            const double a = amp[ib];
+            const size_t d = 2 * ((size_t)k + 2 * ((size_t)i + (size_t)n_energies * (t + tau - 1)));
+            dc_corr[d] += vals[o] / a / n_avg;
+            dc_corr[d + 1] += vals[o + 1] / a / n_avg;
+          }
+  }
+}
+
+// ---- psi(t) -------------------------------------------------------------------
+
+template <typename R>
+void psi_t_run(tbpm_ctx* c, const Expansion& ex, const double* psi0, const int32_t* time_log,
+               int n_log, int n_timestep, int chk_step, double chk_thr, double* psi_t) {
+  constexpr int V = 1;
+  c->graph.reset();
+  ensure_vectors(c, 1, 1);
+  c->out.ensure((size_t)(n_timestep + 1) * 3 * sizeof(double));
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  upload_states<R>(c, psi0, 1, 1, 0, A);
+  reset_counters(c, 0);
+  enqueue_corr<R, V>(c, A, nullptr, 1, 0, c->out.as<double>(), counters(c, 0));
+  const int64_t n = c->ham.n;
+  auto step = [&]() {
+    enqueue_expansion<R, V>(c, ex, 1, A, X, Y, nullptr, 0, c->out.as<double>(), counters(c, 0));
+  };
+  const auto key = plan_key(c, 3, 1, V, ex);
+  const double thr = effective_thr(c, chk_thr);
+  std::vector<double> host;
+  int done = 0;  // steps enqueued
+  int ptr = 0;
+  // tbpm.f90:1071-1092: at iteration t the state after t-1 steps is logged if
+  // requested, checked at t == chk_step, then propagated.
+  auto advance_to = [&](int target) {
+    if (target > done) {
+      run_steps(c, target - done, key, step);
+      done = target;
+    }
+  };
+  for (int t = 1; t <= n_timestep; ++t) {
+    if (ptr < n_log && time_log[ptr] == t - 1) {
+      advance_to(t - 1);
+      download_states<R>(c, A, 1, 1, 0, psi_t + 2 * (size_t)ptr * n);
+      if (ptr < n_log - 1) ++ptr;
+      else ptr = n_log;  // further matches impossible (sorted, unique)
+    }
+    if (t == chk_step) {
+      advance_to(t - 1);
+      read_out(c, host, (size_t)(done + 1) * 3);
+      if (norm_broken(host[(size_t)done * 3 + 2], host[2], thr)) raise_norm("tbpm_psi_t", t);
+    }
+  }
+  if (ptr < n_log && time_log[ptr] == n_timestep) {
+    advance_to(n_timestep);
+    download_states<R>(c, A, 1, 1, 0, psi_t + 2 * (size_t)ptr * n);
+  }
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+}
+
+// ---- Fermi coefficients (funcs.f90:60-123) --------------------------------------
+
+// In-place iterative radix-2 FFT, X_k = sum_n x_n exp(sgn*2*pi*i*k*n/N).
+void fft_radix2(std::vector<double>& re, std::vector<double>& im, int sgn) {
+  const size_t n = re.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      std::swap(re[i], re[j]);
+      std::swap(im[i], im[j]);
+    }
+  }
+  const double pi = 3.14159265358979323846;
+  for (size_t len = 2; len <= n; len <<= 1) {
+    const double ang = sgn * 2 * pi / (double)len;
+    for (size_t i = 0; i < n; i += len) {
+      for (size_t k = 0; k < len / 2; ++k) {
+        const double wr = std::cos(ang * (double)k), wi = std::sin(ang * (double)k);
+        const size_t a = i + k, b = i + k + len / 2;
+        const double tr = re[b] * wr - im[b] * wi;
+        const double ti = re[b] * wi + im[b] * wr;
+        re[b] = re[a] - tr;
+        im[b] = im[a] - ti;
+        re[a] += tr;
+        im[a] += ti;
+      }
+    }
+  }
+}
+
+int fermi_coef(int nr_fermi, double beta, double mu, bool one_minus, double eps,
+               std::vector<double>& coef) {
+  if (nr_fermi < 4 || (nr_fermi & (nr_fermi - 1)))
+    throw Error{TBPM_ERR_ARG, "nr_Fermi_fft_steps must be a power of two >= 4"};
+  const double pi = 3.14159265358979323846;
+  std::vector<double> re(nr_fermi), im(nr_fermi, 0.0);
+  const double r0 = 2 * pi / nr_fermi;
+  for (int i = 0; i < nr_fermi; ++i) {
+    const double e = std::cos(i * r0);
+    double f;  // funcs.f90:36-57
+    if (e >= mu) {
+      const double x = std::exp(beta * (mu - e));
+      f = x / (1 + x);
+    } else {
+      const double x = std::exp(beta * (e - mu));
+      f = 1 / (1 + x);
+    }
+    re[i] = one_minus ? 1.0 - f : f;
+  }
+  fft_radix2(re, im, -1);
+  int n_cheb = nr_fermi / 2;
+  coef.assign(nr_fermi + 1, 0.0);
+  const double q = pi / n_cheb;
+  const double cotq = std::cos(q) / std::sin(q);
+  for (int k = 0; k < n_cheb; ++k) {
+    // Jackson kernel with the first element halved (kpm.f90:8-29)
+    const double g =
+        k == 0 ? 0.5 : ((double)(n_cheb - k) * std::cos(q * k) + cotq * std::sin(q * k)) / n_cheb;
+    coef[k] = g * re[k] / n_cheb;
+  }
+  for (int i = 0; i < n_cheb; ++i) {
+    if (std::fabs(coef[i]) < eps && std::fabs(coef[i + 1]) < eps) {
+      n_cheb = i + 1;
+      break;
+    }
+  }
+  coef.resize(n_cheb);
+  return n_cheb;
+}
+
+// ---- Hamiltonian upload --------------------------------------------------------
+
+void validate_csr(const int32_t* indptr, const int32_t* indices, int64_t n, int64_t nnz) {
+  if (n < 1) throw Error{TBPM_ERR_ARG, "empty Hamiltonian (n_rows < 1)"};
+  if (nnz < 0 || nnz > INT32_MAX) throw Error{TBPM_ERR_ARG, "nnz out of the int32 range"};
+  if (n > INT32_MAX) throw Error{TBPM_ERR_ARG, "n_rows out of the int32 range"};
+  if (indptr[0] != 0) throw Error{TBPM_ERR_ARG, "indptr[0] must be 0"};
+  for (int64_t i = 0; i < n; ++i)
+    if (indptr[i + 1] < indptr[i]) throw Error{TBPM_ERR_ARG, "indptr must be non-decreasing"};
+  if ((int64_t)indptr[n] != nnz) throw Error{TBPM_ERR_ARG, "indptr[n_rows] != nnz"};
+  for (int64_t j = 0; j < nnz; ++j)
+    if (indices[j] < 0 || (int64_t)indices[j] >= n)
+      throw Error{TBPM_ERR_ARG, "column index out of range"};
+}
+
+void upload_real(tbpm_ctx* c, const double* src, int64_t count, DevMem& dst) {
+  const size_t rs = c->opts.precision == TBPM_PREC_FP64 ? 8 : 4;
+  dst.ensure((size_t)std::max<int64_t>(count, 2) * rs);
+  if (count == 0) return;
+  if (rs == 8) {
+    TBPM_CK(cudaMemcpyAsync(dst.p, src, (size_t)count * 8, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    c->stage.ensure((size_t)count * 8);
+    TBPM_CK(cudaMemcpyAsync(c->stage.p, src, (size_t)count * 8, cudaMemcpyHostToDevice,
+                            c->stream));
+    cast_f64_to_f32_kernel<<<blocks_for(count, 256), 256, 0, c->stream>>>(
+        c->stage.as<double>(), count, dst.as<float>());
+    TBPM_CK(cudaGetLastError());
+  }
+}
+
+void ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices, const double* hop,
+                int64_t n, int64_t nnz, const double* dx, const double* dy, double rescale) {
+  validate_csr(indptr, indices, n, nnz);
+  c->graph.reset();
+  c->sess.active = false;
+  Ham& h = c->ham;
+  h.n = 0;
+  h.indptr.ensure((size_t)(n + 1) * 4);
+  h.indices.ensure((size_t)std::max<int64_t>(nnz, 1) * 4);
+  TBPM_CK(cudaMemcpyAsync(h.indptr.p, indptr, (size_t)(n + 1) * 4, cudaMemcpyHostToDevice,
+                          c->stream));
+  if (nnz)
+    TBPM_CK(cudaMemcpyAsync(h.indices.p, indices, (size_t)nnz * 4, cudaMemcpyHostToDevice,
+                            c->stream));
+  upload_real(c, hop, 2 * nnz, h.hop);
+  h.has_dxy = dx && dy;
+  if (h.has_dxy) {
+    upload_real(c, dx, nnz, h.dx);
+    upload_real(c, dy, nnz, h.dy);
+  }
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  h.prec = c->opts.precision;
+  h.n = n;
+  h.nnz = nnz;
+  h.rescale = rescale;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// drivers used by the C ABI
+// ---------------------------------------------------------------------------
+
+void drv_ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
+                    const double* hop, int64_t n, int64_t nnz, const double* dx,
+                    const double* dy, double rescale) {
+  if (!indptr || (nnz > 0 && (!indices || !hop))) throw Error{TBPM_ERR_ARG, "null CSR array"};
+  ham_upload(c, indptr, indices, hop, n, nnz, dx, dy, rescale);
+}
+
+void drv_dos(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
+             int seed, int rank, int n_ran_samples, int n_timestep, int chk_step,
+             double chk_thr, double* corr, double* corr_per_state) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  if (!corr) throw Error{TBPM_ERR_ARG, "null output"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  std::fill(corr, corr + 2 * (size_t)(n_timestep + 1), 0.0);
+  const Expansion ex = time_step_expansion(bes, n_bes);
+  const int B = batch_size(c);
+  for (int s0 = 0; s0 < n_states; s0 += B) {
+    const int ns = std::min(B, n_states - s0);
+    StateKeys keys{};
+    const StateKeys* kp = nullptr;
+    if (!wf0) {
+      keys = make_keys(seed, s0 + 1, ns, rank, n_ran_samples);
+      kp = &keys;
+    }
+    const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
+    dispatch(c->ham.prec, pick_V(c->ham.prec, ns, ns), [&](auto tag) {
+      using P = decltype(tag);
+      dos_batch<typename P::Real, P::V>(c, ex, ns, kp, hw, n_timestep, chk_step, chk_thr,
+                                        n_states, corr, corr_per_state, s0, n_states);
+    });
+  }
+}
+
+void drv_ac(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
+            const double* wf0, int n_states, int seed, int rank, int n_ran_samples,
+            int n_timestep, int nr_fermi, double fermi_precision, int chk_step, double chk_thr,
+            double* corr) {
+  require_ham(c, true);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  std::fill(corr, corr + 2 * 4 * (size_t)n_timestep, 0.0);
+  std::vector<double> cf, comf;
+  const int nf = fermi_coef(nr_fermi, beta, mu, false, fermi_precision, cf);
+  const int nomf = fermi_coef(nr_fermi, beta, mu, true, fermi_precision, comf);
+  if (nf < 3 || nomf < 3) throw Error{TBPM_ERR_ARG, "Fermi expansion shorter than 3 terms"};
+  const Expansion ex_time = time_step_expansion(bes, n_bes);
+  const int B = std::min(batch_size(c), kMaxCols / 3);
+  for (int s0 = 0; s0 < n_states; s0 += B) {
+    const int nb = std::min(B, n_states - s0);
+    unsigned long long set_b = 0;
+    for (int b = 2 * nb; b < 3 * nb; ++b) set_b |= 1ull << b;
+    const Expansion ex_fermi = fermi_expansion(comf.data(), nomf, cf.data(), nf, set_b);
+    StateKeys keys{};
+    const StateKeys* kp = nullptr;
+    if (!wf0) {
+      keys = make_keys(seed, s0 + 1, nb, rank, n_ran_samples);
+      kp = &keys;
+    }
+    const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
+    dispatch(c->ham.prec, pick_V(c->ham.prec, 3 * nb, nb), [&](auto tag) {
+      using P = decltype(tag);
+      ac_batch<typename P::Real, P::V>(c, ex_time, ex_fermi, nb, kp, hw, n_timestep, chk_step,
+                                       chk_thr, n_states, corr);
+    });
+  }
+}
+
+
+void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
+            int seed, int rank, int n_ran_samples, int n_timestep, double t_step,
+            const double* energies, int n_energies, const int32_t* en_inds, int n_en_inds,
+            int chk_step, double chk_thr, double* dos_corr, double* dc_corr) {
+  require_ham(c, true);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  if (n_en_inds < 0 || n_en_inds > n_energies || (n_en_inds > 0 && (!en_inds || !energies)))
+    throw Error{TBPM_ERR_ARG, "bad energy selection"};
+  if (!dos_corr || !dc_corr) throw Error{TBPM_ERR_ARG, "null output"};
+  std::vector<double> en_sel(n_en_inds);
+  for (int i = 0; i < n_en_inds; ++i) {
+    if (en_inds[i] < 0 || en_inds[i] >= n_energies)
+      throw Error{TBPM_ERR_ARG, "energy index out of range"};
+    en_sel[i] = energies[en_inds[i]];
+  }
+  c->launches = 0;
+  c->model_bytes = 0;
+  std::fill(dos_corr, dos_corr + 2 * (size_t)n_timestep, 0.0);
+  std::fill(dc_corr, dc_corr + 2 * 2 * (size_t)n_energies * n_timestep, 0.0);
+  const Expansion ex_fwd = time_step_expansion(bes, n_bes);
+  // states per batch: the QE block (N x n_en x nb complex) must fit in memory
+  int B = std::min(batch_size(c), kMaxCols / 2);
+  {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && n_en_inds > 0) {
+      const size_t per_state = (size_t)c->ham.n * n_en_inds * 2 * real_size(c->ham.prec);
+      const size_t budget = free_b > ((size_t)4 << 30) ? free_b - ((size_t)4 << 30) : free_b / 2;
+      const int fit = (int)std::max<size_t>(1, budget / std::max<size_t>(per_state, 1) / 2);
+      B = std::min(B, fit);
+    }
+    (void)cudaGetLastError();
+  }
+  for (int s0 = 0; s0 < n_states; s0 += B) {
+    const int nb = std::min(B, n_states - s0);
+    Expansion ex_pm = ex_fwd;
+    for (int b = nb; b < 2 * nb; ++b) ex_pm.neg_mask |= 1ull << b;
+    StateKeys keys{};
+    const StateKeys* kp = nullptr;
+    if (!wf0) {
+      keys = make_keys(seed, s0 + 1, nb, rank, n_ran_samples);
+      kp = &keys;
+    }
+    const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
+    dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb), [&](auto tag) {
+      using P = decltype(tag);
+      dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep, t_step, en_sel,
+                                       chk_step, chk_thr, n_states, n_energies, dos_corr,
+                                       dc_corr);
+    });
+  }
+}
+
+void drv_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const double* psi0,
+               const int32_t* time_log, int n_log, int n_timestep, int chk_step,
+               double chk_thr, double* psi_t) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_log < 1 || !time_log) throw Error{TBPM_ERR_ARG, "time_log must not be empty"};
+  for (int i = 0; i < n_log; ++i) {
+    if (time_log[i] < 0 || time_log[i] > n_timestep)
+      throw Error{TBPM_ERR_ARG, "time in time_log out of [0, n_timestep]"};
+    if (i && time_log[i] <= time_log[i - 1])
+      throw Error{TBPM_ERR_ARG, "time_log must be sorted and unique"};
+  }
+  c->launches = 0;
+  c->model_bytes = 0;
+  const Expansion ex = time_step_expansion(bes, n_bes);
+  if (c->ham.prec == TBPM_PREC_FP64)
+    psi_t_run<double>(c, ex, psi0, time_log, n_log, n_timestep, chk_step, chk_thr, psi_t);
+  else
+    psi_t_run<float>(c, ex, psi0, time_log, n_log, n_timestep, chk_step, chk_thr, psi_t);
+}
+
+void drv_random_states(tbpm_ctx* c, int64_t n, int seed, int first_sample, int n_states,
+                       int rank, int n_ran_samples, int kind, double* wf) {
+  if (n < 1 || n_states < 1) throw Error{TBPM_ERR_ARG, "bad sizes"};
+  c->sess.active = false;
+  c->graph.reset();
+  // the generator only needs the row count; use a temporary geometry
+  const int64_t saved_n = c->ham.n;
+  const int saved_prec = c->ham.prec;
+  c->ham.n = n;
+  c->ham.prec = TBPM_PREC_FP64;
+  try {
+    for (int s0 = 0; s0 < n_states; s0 += kMaxCols) {
+      const int ns = std::min(kMaxCols, n_states - s0);
+      const StateKeys keys = make_keys(seed, first_sample + s0, ns, rank, n_ran_samples);
+      c->wf0.ensure((size_t)n * ns * 16);
+      c->ctr.ensure(16 * sizeof(int));
+      gen_states<double, 1>(c, keys, ns, kind, c->wf0.as<Pack<double, 1>>());
+      download_states<double>(c, c->wf0.p, ns, ns, 0, wf + 2 * (size_t)s0 * n);
+    }
+  } catch (...) {
+    c->ham.n = saved_n;
+    c->ham.prec = saved_prec;
+    throw;
+  }
+  c->ham.n = saved_n;
+  c->ham.prec = saved_prec;
+}
+
+void drv_fermi_coef(int nr_fermi, double beta, double mu, int one_minus, double eps,
+                    double* coef, int* n_cheb) {
+  std::vector<double> cf;
+  const int n = fermi_coef(nr_fermi, beta, mu, one_minus != 0, eps, cf);
+  std::fill(coef, coef + nr_fermi, 0.0);
+  std::copy(cf.begin(), cf.end(), coef);
+  *n_cheb = n;
+}
+
+void drv_expansion_apply(tbpm_ctx* c, const Expansion& ex, double* wf, int n_states) {
+  require_ham(c, false);
+  if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
+  c->graph.reset();
+  const int ld = n_states;
+  ensure_vectors(c, ld, 1);
+  dispatch(c->ham.prec, pick_V(c->ham.prec, ld, ld), [&](auto tag) {
+    using P = decltype(tag);
+    using R = typename P::Real;
+    constexpr int V = P::V;
+    upload_states<R>(c, wf, n_states, ld, 0, c->A.p);
+    enqueue_expansion<R, V>(c, ex, ld, c->A.as<Pack<R, V>>(), c->X.as<Pack<R, V>>(),
+                            c->Y.as<Pack<R, V>>(), nullptr, 0, nullptr, Counters{});
+    download_states<R>(c, c->A.p, n_states, ld, 0, wf);
+  });
+}
+
+void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_states, int seed,
+                           int rank, int n_ran_samples, int n_timestep) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  const Expansion ex = time_step_expansion(bes, n_bes);
+  const StateKeys keys = make_keys(seed, 1, n_states, rank, n_ran_samples);
+  dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states), [&](auto tag) {
+    using P = decltype(tag);
+    dos_session_begin<typename P::Real, P::V>(c, ex, n_states, &keys, nullptr, n_timestep + 1);
+  });
+}
+
+void drv_session_advance(tbpm_ctx* c, int n_steps) {
+  if (!c->sess.active) throw Error{TBPM_ERR_STATE, "no session active"};
+  if (n_steps < 0) throw Error{TBPM_ERR_ARG, "n_steps < 0"};
+  dispatch(c->ham.prec, c->sess.V, [&](auto tag) {
+    using P = decltype(tag);
+    dos_session_advance<typename P::Real, P::V>(c, n_steps);
+  });
+}
+
+void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done) {
+  if (!c->sess.active) throw Error{TBPM_ERR_STATE, "no session active"};
+  const int rows = c->sess.rows_enqueued, ld = c->sess.ld;
+  std::vector<double> host;
+  read_out(c, host, (size_t)rows * ld * 3);
+  for (int r = 0; r < rows; ++r)
+    for (int b = 0; b < ld; ++b) {
+      const double* v = &host[((size_t)r * ld + b) * 3];
+      if (corr) {
+        corr[2 * ((size_t)r * ld + b)] = v[0];
+        corr[2 * ((size_t)r * ld + b) + 1] = v[1];
+      }
+      if (norms) norms[(size_t)r * ld + b] = v[2];
+    }
+  if (n_done) *n_done = rows;
+}
+
+}  // namespace tbpm

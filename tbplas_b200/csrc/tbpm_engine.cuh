@@ -1,0 +1,104 @@
+// Host-side engine of libtbpm_b200: device buffers, launch plans, CUDA-graph
+// replay and the drivers behind the C ABI (include/tbpm_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "tbpm_b200.h"
+
+namespace tbpm {
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+void throw_cuda(cudaError_t e, const char* what);
+#define TBPM_CK(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) ::tbpm::throw_cuda(e_, #call); \
+  } while (0)
+
+// Grow-only device allocation.
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t n);
+  void release();
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+};
+
+struct Ham {
+  int prec = -1;
+  int64_t n = 0, nnz = 0;
+  DevMem indptr, indices, hop, dx, dy;
+  bool has_dxy = false;
+  double rescale = 1.0;
+};
+
+// Chebyshev-type expansion  out = sum_k w_k p_k,
+//   p_0 = psi, p_1 = alpha1 * H p_0, p_k = alpha * H p_{k-1} + beta * p_{k-2}.
+struct Expansion {
+  int n_terms = 0;
+  double alpha1_re = 0, alpha1_im = 0;
+  double alpha_re = 0, alpha_im = 0;
+  double beta = 0;
+  std::vector<double> w[2];
+  unsigned long long neg_mask = 0, set_mask = 0;
+};
+
+Expansion time_step_expansion(const double* bes, int n_bes);
+Expansion fermi_expansion(const double* coef_a, int n_a, const double* coef_b, int n_b,
+                          unsigned long long set_b_mask);
+
+struct Tile {
+  int threads = 256;
+  int rpp = 1;
+  int64_t rows_per_tile = 1;
+  int grid = 1;
+};
+
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<unsigned char> key;
+  int steps = 0;
+  void reset();
+  ~GraphCache() { reset(); }
+};
+
+struct Session {
+  bool active = false;
+  int kind = 0;  // 1 = DOS
+  int ld = 0;
+  int V = 1;
+  int rows_cap = 0;
+  int rows_enqueued = 0;
+  Expansion ex;
+};
+
+}  // namespace tbpm
+
+struct tbpm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  tbpm_options opts{};
+  std::string err;
+  tbpm::Ham ham;
+  tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef;
+  int64_t launches = 0;
+  double model_bytes = 0;
+  tbpm::Session sess;
+  tbpm::GraphCache graph;
+};

@@ -1,0 +1,201 @@
+"""Analyzer: correlation functions -> DOS, AC and DC conductivity.
+
+Same API and formulas as tbplas/tbpm/analysis.py (window functions :20-51,
+calc_dos :89-143, calc_ac_cond :161-243, calc_dc_cond :375-458,
+calc_diff_coeff :460-511), with the O(nr_time_steps^2) Python loops of the
+reference replaced by numpy array expressions.  Results agree with the
+reference to floating-point summation order.
+"""
+
+from math import cos, exp, pi
+from typing import Callable, Tuple
+
+import numpy as np
+from scipy.integrate import cumulative_trapezoid
+from scipy.signal import hilbert
+
+from ..parallel import MPIEnv
+from .config import Config
+
+__all__ = ["window_hanning", "window_exp", "window_exp_ten", "Analyzer"]
+
+
+def window_hanning(i: int, tnr: int) -> float:
+    """Hanning window 0.5*(1 + cos(pi*i/tnr))."""
+    return 0.5 * (1 + cos(pi * i / tnr))
+
+
+def window_exp(i: int, tnr: int) -> float:
+    """Exponential window exp(-2*(i/tnr)^2)."""
+    return exp(-2. * (i / tnr)**2)
+
+
+def window_exp_ten(i: int, tnr: int) -> float:
+    """Exponential window 10^(-2*(i/tnr)^2)."""
+    power = -2 * (1. * i / tnr)**2
+    return 10.**power
+
+
+def _window_values(window: Callable, start: int, stop: int, tnr: int) -> np.ndarray:
+    return np.array([window(i, tnr) for i in range(start, stop)], dtype=float)
+
+
+class Analyzer(MPIEnv):
+    """Post-processing of TBPM correlation functions (see tbplas.tbpm.Analyzer)."""
+
+    def __init__(self, sample, config: Config, dimension: int = 3,
+                 enable_mpi: bool = False, echo_details: bool = False) -> None:
+        super().__init__(enable_mpi=enable_mpi, echo_details=echo_details)
+        self._sample = sample
+        self._config = config
+        self._config.check_params()
+        if dimension not in (2, 3):
+            raise ValueError(f"Unsupported dimension: {dimension}")
+        self._dimension = dimension
+
+    def _energies(self) -> np.ndarray:
+        tnr = self._config.generic['nr_time_steps']
+        en_range = self._sample.energy_range
+        return np.array([0.5 * i * en_range / tnr - en_range / 2. for i in range(tnr * 2)],
+                        dtype=float)
+
+    def calc_dos(self, corr_dos: np.ndarray,
+                 window: Callable = window_hanning) -> Tuple[np.ndarray, np.ndarray]:
+        """DOS from the DOS correlation function (analysis.py:89-143).
+
+        :return: (energies, dos), both (2*nr_time_steps,) float64
+        """
+        tnr = self._config.generic['nr_time_steps']
+        en_range = self._sample.energy_range
+        en_step = 0.5 * en_range / tnr
+        energies = self._energies()
+        dos = np.zeros(tnr * 2, dtype=float)
+        if self.is_master:
+            c = np.asarray(corr_dos, dtype=complex).reshape(-1)
+            w = _window_values(window, 0, tnr, tnr)
+            neg = np.empty(tnr * 2, dtype=complex)
+            neg[tnr - 1] = c[0]
+            neg[2 * tnr - 1] = w[tnr - 1] * c[tnr]
+            neg[tnr:2 * tnr - 1] = w[:tnr - 1] * c[1:tnr]
+            neg[tnr - 2::-1] = w[:tnr - 1] * np.conj(c[1:tnr])
+            fft = np.abs(np.fft.ifft(neg))
+            dos[tnr:] = fft[:tnr]
+            dos[:tnr] = fft[tnr:]
+            dos = dos / (np.sum(dos) * en_step)
+            if self._config.generic['correct_spin']:
+                dos = 2. * dos
+        self.bcast(dos)
+        return energies, dos
+
+    def calc_ldos(self, corr_ldos: np.ndarray,
+                  window: Callable = window_hanning) -> Tuple[np.ndarray, np.ndarray]:
+        """LDOS from the LDOS correlation function."""
+        return self.calc_dos(corr_ldos, window)
+
+    def calc_ac_cond(self, corr_ac: np.ndarray,
+                     window: Callable = window_exp) -> Tuple[np.ndarray, np.ndarray]:
+        """AC conductivity from its correlation function (analysis.py:161-243).
+
+        :return: (omegas, ac_cond): (nr_time_steps,) float64 and
+            (4, nr_time_steps) complex128 (xx, xy, yx, yy)
+        """
+        tnr = self._config.generic['nr_time_steps']
+        en_range = self._sample.energy_range
+        t_step = pi / en_range
+        beta = self._config.generic['beta']
+        if self._dimension == 2:
+            prefactor = self._sample.nr_orbitals / (self._sample.area_unit_cell *
+                                                    self._sample.extended)
+        else:
+            prefactor = self._sample.nr_orbitals / (self._sample.volume_unit_cell *
+                                                    self._sample.extended)
+        omegas = np.array([i * en_range / tnr for i in range(tnr)], dtype=float)
+        ac_cond = np.zeros((4, tnr), dtype=complex)
+        if self.is_master:
+            corr = np.asarray(corr_ac)
+            w = _window_values(window, 1, tnr + 1, tnr)
+            k = np.arange(tnr, dtype=float)
+            # S[i, k] = 2 w(k+1) sin(omega_i k dt)
+            s = 2. * w[None, :] * np.sin(np.outer(omegas, k) * t_step)
+            acv = s @ np.imag(corr[:, :tnr]).T  # (tnr, 4)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                fac = prefactor * t_step * (np.exp(-beta * omegas) - 1) / omegas
+            fac[omegas == 0.] = 0.
+            ac_real = (acv * fac[:, None]).T
+            ac_real[:, omegas == 0.] = 0.
+            ac_imag = np.zeros((4, tnr), dtype=float)
+            for j in range(4):
+                sigma = np.zeros(2 * tnr, dtype=float)
+                sigma[tnr:] = ac_real[j]
+                sigma[tnr - np.arange(tnr)] = ac_real[j]
+                ac_imag[j, :] = np.imag(hilbert(sigma))[tnr:2 * tnr]
+            ac_cond = ac_real + 1j * ac_imag
+            if self._config.generic['correct_spin']:
+                ac_cond = 2. * ac_cond
+        self.bcast(ac_cond)
+        return omegas, ac_cond
+
+    def _qe_window(self):
+        tnr = self._config.generic['nr_time_steps']
+        energies = self._energies()
+        en_limit = self._config.DC_conductivity['energy_limits']
+        qe_indices = np.where((energies >= en_limit[0]) & (energies <= en_limit[1]))[0]
+        return tnr, energies, qe_indices
+
+    def calc_dc_cond(self, corr_dos: np.ndarray, corr_dc: np.ndarray,
+                     window_dos: Callable = window_hanning,
+                     window_dc: Callable = window_exp) -> Tuple[np.ndarray, np.ndarray]:
+        """Zero-temperature DC conductivity (analysis.py:375-458).
+
+        :return: (energies, dc): (n_energies,) float64 and (2, n_energies) float64
+        """
+        corr_dos = np.insert(np.asarray(corr_dos), 0, 1.0)
+        _, dos = self.calc_dos(corr_dos, window_dos)
+        tnr, energies_dos, qe_indices = self._qe_window()
+        en_range = self._sample.energy_range
+        t_step = 2 * pi / en_range
+        n_energies = len(qe_indices)
+        energies = energies_dos[qe_indices]
+        if self._dimension == 2:
+            prefactor = self._sample.nr_orbitals / self._sample.area_unit_cell
+        else:
+            prefactor = self._sample.nr_orbitals / self._sample.volume_unit_cell
+        dc = np.zeros((2, n_energies))
+        if self.is_master:
+            w = _window_values(window_dc, 1, tnr + 1, tnr)
+            k = np.arange(tnr, dtype=float)
+            phi = np.outer(energies, k) * t_step  # (n_en, tnr)
+            c_exp = np.cos(phi) - 1j * np.sin(phi)
+            corr = np.asarray(corr_dc)[:, :n_energies, :tnr]
+            vals = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
+            dc_val = vals.sum(axis=2)
+            dc = prefactor * t_step * dos[qe_indices][None, :] * dc_val
+            if self._config.generic['correct_spin']:
+                dc = 2. * dc
+        self.bcast(dc)
+        return energies, dc
+
+    def calc_diff_coeff(self, corr_dc: np.ndarray,
+                        window_dc: Callable = window_exp) -> Tuple[np.ndarray, np.ndarray]:
+        """Diffusion coefficient from the DC correlation (analysis.py:460-511).
+
+        :return: (time, diff_coeff): (nr_time_steps,) float64 and
+            (2, n_energies, nr_time_steps) float64
+        """
+        tnr, energies_dos, qe_indices = self._qe_window()
+        en_range = self._sample.energy_range
+        t_step = 2 * pi / en_range
+        n_energies = len(qe_indices)
+        energies = energies_dos[qe_indices]
+        time = np.linspace(0, tnr - 1, tnr) * t_step
+        diff_coeff = np.zeros((2, n_energies, tnr))
+        if self.is_master:
+            w = _window_values(window_dc, 1, tnr + 1, tnr)
+            k = np.arange(tnr, dtype=float)
+            phi = np.outer(energies, k) * t_step
+            c_exp = np.cos(phi) - 1j * np.sin(phi)
+            corr = np.asarray(corr_dc)[:, :n_energies, :tnr]
+            temp = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
+            diff_coeff[:, :, 1:] = cumulative_trapezoid(temp, time, axis=2)
+        self.bcast(diff_coeff)
+        return time, diff_coeff
