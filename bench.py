@@ -1,0 +1,436 @@
+"""Benchmark of the TBPM hot path on B200.
+
+Workload (the headline configuration): graphene 2048 x 2048 periodic
+supercell (8,388,608 orbitals), t = -2.7 eV, Anderson on-site disorder
+U[-0.5, 0.5] eV, rescale 9 eV (nnz = 33.5M), 16 random-phase states
+propagated as one block; one bench step = one TBPM time step of the DOS
+correlation (19 Chebyshev terms + the fused correlation) for the whole block.
+
+  value   orbital-steps/s on the device (state block and Hamiltonian resident
+          in HBM), CUDA events on the library stream, max over ranks
+  e2e     the same metric through the public API f2py.tbpm_dos (host CSR and
+          host result buffers; uploads, state generation, propagation and the
+          result download inside the timed region)
+  roofline  algorithmic HBM bytes of the Chebyshev-term kernel family per
+          step / measured step time, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C++/OpenMP restatement of the reference
+          Fortran) on this host's cores, bounded sample of the same workload
+
+`--impl reference` times the CPU oracle alone (the reference Fortran cannot be
+built on this image) and prints its own JSON line.
+
+Multi-GPU (torchrun): every rank propagates its own 16 states (weak scaling,
+the reference's random-sample decomposition); the correlation arrays are
+averaged with one all_reduce at the end of the e2e call.
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 2048
+N_STATES = 16
+DISORDER_W = 1.0
+RESCALE = 9.0
+SEED = 1337
+HBM_FALLBACK_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def bessel_series(time_scaled, precision=1e-14):
+    import scipy.special as spec
+    out = []
+    for i in range(250):
+        v = spec.jv(i, time_scaled)
+        if abs(v) > precision or abs(spec.jv(i + 1, time_scaled)) > precision:
+            out.append(float(v))
+        else:
+            return out
+    raise ValueError("Bessel_max too low")
+
+
+def build_sample():
+    import tbplas_b200 as tb
+    t0 = time.time()
+    s = tb.make_graphene_sample(NX, NY, disorder=DISORDER_W, rescale=RESCALE, seed=SEED)
+    h = s.build_ham_csr()
+    log(f"[bench] built {NX}x{NY} graphene: N={h.shape[0]} nnz={h.nnz} in {time.time() - t0:.1f}s")
+    return s, h
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"tbpm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.remove(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes):
+    """HBM bytes one time step of the fused kernel family must move.
+
+    Per Chebyshev term k = 1..n_bes-1 the kernel reads the CSR once
+    ((n+1)*4 + nnz*(4 + 2*real_bytes)) and the gathered vector p_{k-1} once
+    (neighbour rows come from L2), reads p_{k-2} and writes p_k (not on the
+    first and last term), and every third term flushes the accumulator
+    (read + write; write only on the first flush); the last term also reads
+    the correlation reference.  This mirrors the kernel schedule of
+    tbplas_b200/csrc/tbpm_engine.cu (enqueue_expansion).
+    """
+    sv = 2 * real_bytes
+    vec = n * ld * sv
+    mat = (n + 1) * 4 + nnz * (4 + sv)
+    total = 0.0
+    last_flush = -1
+    for k in range(1, n_bes):
+        b = mat + vec
+        if k == 1:
+            b += vec
+        else:
+            b += vec * (2 if k < n_bes - 1 else 1)
+            pending = k - last_flush
+            if k == 2 or pending == 3 or k == n_bes - 1:
+                b += vec * (1 if k == 2 else 2)
+                last_flush = k
+        if k == n_bes - 1:
+            b += vec  # correlation reference wf0
+        total += b
+    return total
+
+
+def survey_model_bytes_per_orbital_step(n, nnz, ld, n_bes, real_bytes):
+    """The 5-passes-per-term byte model (M + B*5*S_v*N per term + S_v)."""
+    sv = 2 * real_bytes
+    m = n * (nnz / n) * (sv + 4) + 4 * (n + 1)
+    return ((n_bes - 1) * (m / (n * ld) + 5 * sv) + sv)
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from tbplas_b200 import _native as nat
+    from tbplas_b200.fortran import f2py
+    from tbplas_b200.parallel import init_distributed
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    distributed = world > 1
+    if distributed:
+        init_distributed(backend="nccl", timeout_s=300)
+    torch.cuda.set_device(local)
+    peak, peak_kind = measured_peak()
+
+    sample, h = build_sample()
+    n, nnz = h.shape[0], h.nnz
+    ip = h.indptr.astype(np.int32)
+    ix = h.indices.astype(np.int32)
+    hv = np.ascontiguousarray(h.data)
+    bes = np.asarray(bessel_series(2 * math.pi / sample.energy_range * sample.rescale))
+    n_bes = bes.size
+
+    ctx = nat.get_context(local)
+    results = {}
+    for prec_name, prec in (("fp64", nat.PREC_FP64), ("fp32", nat.PREC_FP32)):
+        if prec_name == "fp32" and args.skip_fp32:
+            continue
+        ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=16)
+        ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, None, None,
+                 sample.rescale)
+        total = args.steps + args.warmup
+        ctx.call("tbpm_session_dos_begin", nat.ptr(bes), n_bes, N_STATES, SEED, rank, N_STATES,
+                 total)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        ctx.call("tbpm_session_advance", args.warmup)
+        torch.cuda.synchronize()
+        if distributed:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if (rank == 0 and prec_name == "fp64") else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        l0, b0 = ctx.last_stats()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ctx.call("tbpm_session_advance", args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        l1, b1 = ctx.last_stats()
+        if distributed:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        ms = ev0.elapsed_time(ev1)
+        if distributed:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        ms_step = ms / args.steps
+        launches = (l1 - l0)
+        model_bytes_step = (b1 - b0) / args.steps
+        rb = 8 if prec == nat.PREC_FP64 else 4
+        alg = algorithmic_bytes_per_step(n, nnz, N_STATES, n_bes, rb)
+        # parity spot check of the session against its own first rows
+        corr = np.zeros((total + 1, N_STATES), dtype=np.complex128)
+        norms = np.zeros((total + 1, N_STATES))
+        import ctypes
+        nd = ctypes.c_int(0)
+        ctx.call("tbpm_session_read", nat.ptr(corr), nat.ptr(norms), ctypes.byref(nd))
+        results[prec_name] = {
+            "ms_per_step": ms_step,
+            "orbital_steps_per_s": n * N_STATES * world / (ms_step * 1e-3),
+            "launches": launches,
+            "alg_bytes_per_step": alg,
+            "lib_model_bytes_per_step": model_bytes_step,
+            "achieved_gbs": alg / (ms_step * 1e-3) / 1e9,
+            "norm_drift": float(np.max(np.abs(norms[:nd.value] - norms[0]))),
+            "clocks": clocks,
+        }
+        log(f"[bench] {prec_name}: {ms_step:.3f} ms/step, "
+            f"{results[prec_name]['orbital_steps_per_s']:.3e} orbital-steps/s, "
+            f"{results[prec_name]['achieved_gbs']:.0f} GB/s, launches {launches}")
+
+    # ---- e2e through the public API (FP64, host buffers) -----------------
+    f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True)
+    from tbplas_b200.parallel import MPIEnv
+    env = MPIEnv(enable_mpi=distributed)
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    if distributed:
+        dist.barrier()
+    t0 = time.perf_counter()
+    corr = f2py.tbpm_dos(bes, ip, ix, hv, SEED, e2e_steps, N_STATES, "unused", rank, 128, 1e-9)
+    corr = env.all_average(corr)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if distributed:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    h2d = ip.nbytes + ix.nbytes + hv.nbytes + bes.nbytes
+    d2h = corr.nbytes
+    e2e = {"value": n * N_STATES * e2e_steps * world / t_e2e, "unit": "orbital-steps/s",
+           "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+           "steps": e2e_steps, "seconds": t_e2e,
+           "note": "one f2py.tbpm_dos call of `steps` time steps: CSR upload and "
+                   "validation, state generation, propagation, result download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline(ip, ix, hv, bes, args.cpu_steps)
+
+    if rank == 0:
+        r64 = results["fp64"]
+        line = {
+            "metric": "orbital-steps/s (TBPM DOS time step, FP64)",
+            "value": r64["orbital_steps_per_s"],
+            "unit": "orbital-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": r64["ms_per_step"],
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64 (complex128 states, SpMV and reductions)",
+            "data": "synthetic: graphene supercell with seeded Anderson disorder and "
+                    "seeded Philox random-phase states",
+            "config": {"workload": "graphene 2048x2048 PBC, W=1 eV Anderson disorder, "
+                                   "16 states as one block, corr_dos time step",
+                       "n_orbitals": n, "nnz": nnz, "states_per_gpu": N_STATES,
+                       "bessel_terms": n_bes, "rescale_eV": RESCALE,
+                       "l2": "inputs larger than L2 (state block 2.1 GB FP64)",
+                       "parallelism": f"replicas of independent state blocks x{world}"},
+            "roofline": {
+                "bound": "hbm",
+                "achieved": r64["achieved_gbs"],
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": r64["achieved_gbs"] / peak,
+                "peak_kind": peak_kind,
+                "traffic": None,
+                "alg_bytes_per_step": r64["alg_bytes_per_step"],
+                "kernel": "cheb_term_kernel<double,1> (+ finalize_kernel, <1% of step)",
+            },
+            "e2e": e2e,
+            "gpu_launches": int(r64["launches"]),
+            "clocks": r64["clocks"],
+            "fp32": {k: results["fp32"][k] for k in ("ms_per_step", "orbital_steps_per_s",
+                                                      "achieved_gbs", "alg_bytes_per_step")}
+            if "fp32" in results else None,
+            "cpu_baseline": cpu,
+        }
+        if "fp32" in results:
+            line["fp32"]["roofline_frac"] = results["fp32"]["achieved_gbs"] / peak
+        print(json.dumps(line), flush=True)
+    if distributed:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(ip, ix, hv, bes, steps):
+    """The oracle (C++/OpenMP restatement of the reference Fortran) on all host
+    cores: 1 random state of the same Hamiltonian, `steps` time steps."""
+    from oracle import oracle
+    L = oracle.lib(native=True)
+    import ctypes
+    threads = os.cpu_count() or 1
+    L.orc_set_threads(threads)
+    n = ip.size - 1
+    wf0 = np.ascontiguousarray(oracle.random_state(n, SEED, 0)[None, :])
+    corr = np.zeros(steps + 1, dtype=np.complex128)
+    b = np.ascontiguousarray(bes)
+    t0 = time.perf_counter()
+    rc = L.orc_tbpm_dos(b.ctypes.data, b.size, ip.ctypes.data, ix.ctypes.data, hv.ctypes.data,
+                        n, wf0.ctypes.data, SEED, steps, 1, 0, 0, 1e-9, 0, corr.ctypes.data)
+    dt = time.perf_counter() - t0
+    if rc != 0:
+        return None
+    return {"value": n * steps / dt, "unit": "orbital-steps/s", "cores": threads,
+            "kind": "port",
+            "sample": f"1 state x {steps} time steps of the 2048x2048 disordered graphene "
+                      f"Hamiltonian (the benchmark uses 16 states per GPU), {dt:.1f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    sample, h = build_sample()
+    ip = h.indptr.astype(np.int32)
+    ix = h.indices.astype(np.int32)
+    hv = np.ascontiguousarray(h.data)
+    n = ip.size - 1
+    bes = np.asarray(bessel_series(2 * math.pi / sample.energy_range * sample.rescale))
+    L = oracle.lib(native=True)
+    threads = os.cpu_count() or 1
+    L.orc_set_threads(threads)
+    wf0 = np.ascontiguousarray(oracle.random_state(n, SEED, 0)[None, :])
+    # one step of the reference arm = one time step of one state
+    corr = np.zeros(args.steps + args.warmup + 1, dtype=np.complex128)
+    L.orc_tbpm_dos(bes.ctypes.data, bes.size, ip.ctypes.data, ix.ctypes.data, hv.ctypes.data,
+                   n, wf0.ctypes.data, SEED, args.warmup, 1, 0, 0, 1e-9, 0, corr.ctypes.data)
+    t0 = time.perf_counter()
+    L.orc_tbpm_dos(bes.ctypes.data, bes.size, ip.ctypes.data, ix.ctypes.data, hv.ctypes.data,
+                   n, wf0.ctypes.data, SEED, args.steps, 1, 0, 0, 1e-9, 0, corr.ctypes.data)
+    dt = time.perf_counter() - t0
+    value = n * args.steps / dt
+    line = {
+        "impl": "reference",
+        "metric": "orbital-steps/s (TBPM DOS time step, FP64)",
+        "value": value,
+        "unit": "orbital-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (complex128)",
+        "data": "synthetic: graphene supercell with seeded Anderson disorder",
+        "config": {"workload": "graphene 2048x2048 PBC, W=1 eV Anderson disorder, "
+                               "corr_dos time step (1 state per step on the CPU)",
+                   "n_orbitals": n, "nnz": int(ix.size)},
+        "cpu_baseline": {"value": value, "unit": "orbital-steps/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"1 state x {args.steps} time steps (reference Fortran "
+                                   f"not buildable here: C++/OpenMP restatement)"},
+        "e2e": {"value": value, "unit": "orbital-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--nx", type=int, default=2048,
+                    help="cells along a1 (smaller values only for profiling captures)")
+    ap.add_argument("--ny", type=int, default=2048)
+    args = ap.parse_args()
+    global NX, NY
+    NX, NY = args.nx, args.ny
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -54,6 +54,41 @@ __device__ __forceinline__ Pack<float, 1> ldg_pack(const Pack<float, 1>* p) {
   return r;
 }
 
+// Streaming (evict-first) access for vectors read or written once per kernel,
+// so they do not push the gathered vector out of L2.
+__device__ __forceinline__ Pack<double, 1> ldcs_pack(const Pack<double, 1>* p) {
+  const double2 d = __ldcs(reinterpret_cast<const double2*>(p));
+  Pack<double, 1> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  return r;
+}
+__device__ __forceinline__ Pack<float, 2> ldcs_pack(const Pack<float, 2>* p) {
+  const float4 d = __ldcs(reinterpret_cast<const float4*>(p));
+  Pack<float, 2> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  r.v[2] = d.z;
+  r.v[3] = d.w;
+  return r;
+}
+__device__ __forceinline__ Pack<float, 1> ldcs_pack(const Pack<float, 1>* p) {
+  const float2 d = __ldcs(reinterpret_cast<const float2*>(p));
+  Pack<float, 1> r;
+  r.v[0] = d.x;
+  r.v[1] = d.y;
+  return r;
+}
+__device__ __forceinline__ void stcs_pack(Pack<double, 1>* p, const Pack<double, 1>& v) {
+  __stcs(reinterpret_cast<double2*>(p), make_double2(v.v[0], v.v[1]));
+}
+__device__ __forceinline__ void stcs_pack(Pack<float, 2>* p, const Pack<float, 2>& v) {
+  __stcs(reinterpret_cast<float4*>(p), make_float4(v.v[0], v.v[1], v.v[2], v.v[3]));
+}
+__device__ __forceinline__ void stcs_pack(Pack<float, 1>* p, const Pack<float, 1>& v) {
+  __stcs(reinterpret_cast<float2*>(p), make_float2(v.v[0], v.v[1]));
+}
+
 __device__ __forceinline__ double2 ldg_c(const double2* p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldg_c(const float2* p) { return __ldg(p); }
 

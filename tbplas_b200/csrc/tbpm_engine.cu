@@ -109,26 +109,63 @@ void dispatch(int prec, int V, F&& f) {
 
 inline size_t real_size(int prec) { return prec == TBPM_PREC_FP64 ? 8 : 4; }
 
-Tile pick_tile(const tbpm_ctx* c, int64_t n_rows, int tpr) {
+int num_sms(int device) {
+  static int cached[64] = {0};
+  if (device < 0 || device >= 64) return kSMs;
+  if (!cached[device]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        v <= 0) {
+      (void)cudaGetLastError();
+      v = kSMs;
+    }
+    cached[device] = v;
+  }
+  return cached[device];
+}
+
+// Resident blocks per SM of `kernel` at the given block shape (cached).
+template <class K>
+int resident_per_sm(K kernel, int threads, size_t smem) {
+  static std::vector<std::pair<std::pair<const void*, long long>, int>> cache;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  const long long shape = (long long)threads * (1ll << 32) + (long long)smem;
+  for (const auto& e : cache)
+    if (e.first.first == key && e.first.second == shape) return e.second;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    nb = 1;
+  }
+  nb = std::max(nb, 1);
+  cache.push_back({{key, shape}, nb});
+  return nb;
+}
+
+// Block shape (threads = rpp rows x tpr threads per row) and a persistent
+// grid: at most the number of blocks that are resident at once, so that the
+// grid-stride kernels sweep the rows as one narrow band.  A positive
+// opts.rows_per_tile instead sizes the grid as ceil(n_rows / rows_per_tile)
+// (for tuning experiments).
+template <class K>
+Tile pick_tile(const tbpm_ctx* c, int64_t n_rows, int tpr, K kernel, size_t smem_per_thread) {
   Tile t;
   int want = c->opts.threads_per_block > 0 ? c->opts.threads_per_block : 256;
-  want = std::min(std::max(want, 32), 512);
+  want = std::min(std::max(want, 32), 256);  // the kernels are bounded to 256 threads
   t.rpp = std::max(1, want / tpr);
-  while (t.rpp * tpr > 512 && t.rpp > 1) --t.rpp;
+  while (t.rpp * tpr > 256 && t.rpp > 1) --t.rpp;
   t.threads = t.rpp * tpr;
-  int64_t passes;
+  const int64_t n_tiles = (n_rows + t.rpp - 1) / t.rpp;
+  int64_t grid;
   if (c->opts.rows_per_tile > 0) {
-    passes = std::max<int64_t>(1, c->opts.rows_per_tile / t.rpp);
+    grid = (n_rows + c->opts.rows_per_tile - 1) / c->opts.rows_per_tile;
   } else {
-    // aim at >= 16 resident-block waves of work while keeping the partial
-    // sums small
-    const int64_t target_blocks = (int64_t)kSMs * 16;
-    passes = n_rows / ((int64_t)t.rpp * target_blocks);
-    passes = std::min<int64_t>(std::max<int64_t>(passes, 1), 64);
+    const int per_sm = resident_per_sm(kernel, t.threads, smem_per_thread * t.threads);
+    grid = (int64_t)per_sm * num_sms(c->device);
   }
-  t.rows_per_tile = (int64_t)t.rpp * passes;
-  t.grid = (int)((n_rows + t.rows_per_tile - 1) / t.rows_per_tile);
-  if (t.grid < 1) t.grid = 1;
+  grid = std::min<int64_t>(std::max<int64_t>(grid, 1), std::max<int64_t>(n_tiles, 1));
+  t.grid = (int)grid;
+  t.rows_per_tile = t.rpp;
   return t;
 }
 
@@ -191,16 +228,45 @@ void launch_finalize(tbpm_ctx* c, int grid_parts, int n_values, Counters k, doub
   c->launches++;
 }
 
+// Block partials of the fused reductions.  A persistent grid needs at most
+// 192 values x (32 blocks per SM x SMs); reserving that much up front keeps
+// every later request inside the buffer, so no allocation happens while a
+// CUDA graph is being captured.
 void ensure_partials(tbpm_ctx* c, size_t n_doubles) {
-  c->partials.ensure(std::max<size_t>(n_doubles, 64) * sizeof(double));
+  const size_t floor_doubles = (size_t)192 * 32 * num_sms(c->device);
+  c->partials.ensure(std::max(n_doubles, floor_doubles) * sizeof(double));
 }
 
+// Launch shapes of the three compiled modes of cheb_term_kernel.
+struct TermTiles {
+  Tile t[3];
+};
+
 template <typename R, int V>
-void launch_term(tbpm_ctx* c, const Tile& t, const TermArgs<R, V>& a) {
-  const size_t smem = a.partials ? (size_t)t.threads * V * 3 * sizeof(double) : 0;
-  cheb_term_kernel<R, V><<<t.grid, t.threads, smem, c->stream>>>(a);
+TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr) {
+  TermTiles tt;
+  tt.t[0] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 0>, 0);
+  tt.t[1] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 1>, 0);
+  tt.t[2] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 2>, V * 3 * sizeof(double));
+  return tt;
+}
+
+// Returns the grid of the launch (needed by the finalize of mode 2).
+template <typename R, int V>
+int launch_term(tbpm_ctx* c, const TermTiles& tt, const TermArgs<R, V>& a) {
+  const int mode = a.partials ? 2 : (a.c.nflush > 0 ? 1 : 0);
+  const Tile& t = tt.t[mode];
+  if (mode == 2) {
+    const size_t smem = (size_t)t.threads * V * 3 * sizeof(double);
+    cheb_term_kernel<R, V, 2><<<t.grid, t.threads, smem, c->stream>>>(a);
+  } else if (mode == 1) {
+    cheb_term_kernel<R, V, 1><<<t.grid, t.threads, 0, c->stream>>>(a);
+  } else {
+    cheb_term_kernel<R, V, 0><<<t.grid, t.threads, 0, c->stream>>>(a);
+  }
   TBPM_CK(cudaGetLastError());
   c->launches++;
+  return t.grid;
 }
 
 // Enqueue one expansion (one time step, or one Fermi operator) on the block A.
@@ -214,9 +280,10 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
   if (!A_out) A_out = A;
   const Ham& h = c->ham;
   const int tpr = ld / V;
-  const Tile t = pick_tile(c, h.n, tpr);
+  const TermTiles tt = term_tiles<R, V>(c, h.n, tpr);
   const bool want = partials_out != nullptr;
-  if (want) ensure_partials(c, (size_t)ld * 3 * t.grid);
+  if (want) ensure_partials(c, (size_t)ld * 3 * tt.t[2].grid);
+  int last_grid = 0;
   auto buf = [&](int k) { return (k & 1) ? X : Y; };
   const int n = ex.n_terms;
   int last_flush = -1;
@@ -229,7 +296,7 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
     a.indices = h.indices.as<int32_t>();
     a.hop = h.hop.as<typename Cx<R>::t>();
     a.n_rows = h.n;
-    a.rows_per_tile = t.rows_per_tile;
+    a.rows_per_tile = tt.t[0].rows_per_tile;
     a.tpr = tpr;
     a.c.neg_mask = ex.neg_mask;
     a.c.set_mask = ex.set_mask;
@@ -272,17 +339,17 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
       a.partials = c->partials.as<double>();
       if (ref) bytes += (double)h.n * ref_ld * sv;
     }
-    launch_term<R, V>(c, t, a);
+    last_grid = launch_term<R, V>(c, tt, a);
     c->model_bytes += bytes;
   }
-  if (want) launch_finalize(c, t.grid, ld * 3, k_ctr, partials_out);
+  if (want) launch_finalize(c, last_grid, ld * 3, k_ctr, partials_out);
 }
 
 template <typename R, int V>
 void enqueue_corr(tbpm_ctx* c, const Pack<R, V>* x, const Pack<R, V>* ref, int ld, int ref_ld,
                   double* out, Counters k_ctr) {
   const int tpr = ld / V;
-  const Tile t = pick_tile(c, c->ham.n, tpr);
+  const Tile t = pick_tile(c, c->ham.n, tpr, corr_kernel<R, V>, V * 3 * sizeof(double));
   ensure_partials(c, (size_t)ld * 3 * t.grid);
   const size_t smem = (size_t)t.threads * V * 3 * sizeof(double);
   corr_kernel<R, V><<<t.grid, t.threads, smem, c->stream>>>(
@@ -297,7 +364,7 @@ void enqueue_corr(tbpm_ctx* c, const Pack<R, V>* x, const Pack<R, V>* ref, int l
 template <typename R, int V>
 void gen_states(tbpm_ctx* c, const StateKeys& keys, int ld, int kind, Pack<R, V>* dst) {
   const int tpr = ld / V;
-  const Tile t = pick_tile(c, c->ham.n, tpr);
+  const Tile t = pick_tile(c, c->ham.n, tpr, gen_state_kernel<R, V>, V * sizeof(double));
   ensure_partials(c, (size_t)ld * t.grid);
   c->small.ensure(sizeof(double) * kMaxCols * 2);
   reset_counters(c, 1);
@@ -627,7 +694,7 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
   c->launches++;
   // Fermi operators (tbpm.f90:279-281): 1-F on the current columns, F on wf0
   enqueue_expansion<R, V>(c, ex_fermi, ld, A, X, Y, nullptr, 0, nullptr, Counters{});
-  const Tile tj = pick_tile(c, h.n, nb);
+  const Tile tj = pick_tile(c, h.n, nb, jcorr_kernel<R>, 9 * sizeof(double));
   const size_t smem_j = (size_t)tj.threads * 9 * sizeof(double);
   reset_counters(c, 0);
   auto jcorr = [&]() {

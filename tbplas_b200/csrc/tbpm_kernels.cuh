@@ -40,7 +40,7 @@ struct TermArgs {
   const int32_t* indices;
   const typename Cx<R>::t* hop;
   int64_t n_rows;
-  int64_t rows_per_tile;
+  int64_t rows_per_tile;  // unused by the grid-stride kernels (kept for layout)
   int tpr;  // threads (packs) per row = ld / V
   const Pack<R, V>* gather;  // p_{k-1}
   const Pack<R, V>* pin;     // p_{k-2} (null when beta == 0)
@@ -52,89 +52,129 @@ struct TermArgs {
   TermCoef c;
 };
 
-template <typename R, int V>
-__global__ void __launch_bounds__(512) cheb_term_kernel(const TermArgs<R, V> a) {
+// Kernel modes: 0 = recurrence only, 1 = recurrence + accumulator flush,
+// 2 = flush + correlation/norm partials (last term of a time step).  Each
+// mode is compiled separately so the common mode-0 terms keep few registers.
+// Blocks have at most 256 threads; the minimum resident blocks per SM bound
+// the registers per thread (4 blocks: 64 registers, 5 blocks: 51).
+#ifndef TBPM_MINB_PLAIN
+#define TBPM_MINB_PLAIN 4
+#endif
+#ifndef TBPM_MINB_FLUSH
+#define TBPM_MINB_FLUSH 4
+#endif
+// neighbours gathered per batch (independent loads in flight per thread)
+#ifndef TBPM_BW_PLAIN
+#define TBPM_BW_PLAIN 4
+#endif
+#ifndef TBPM_BW_FLUSH
+#define TBPM_BW_FLUSH 2
+#endif
+
+template <typename R, int V, int MODE>
+__global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_FLUSH))
+    cheb_term_kernel(const TermArgs<R, V> a) {
   extern __shared__ double smem[];
   const int tpr = a.tpr;
   const int slot = threadIdx.x / tpr;
   const int lane = threadIdx.x - slot * tpr;
   const int rpp = blockDim.x / tpr;
-  const int64_t r0 = (int64_t)blockIdx.x * a.rows_per_tile;
-  const int64_t r1 = min(r0 + a.rows_per_tile, a.n_rows);
+  // Persistent grid-stride schedule over row tiles of rpp rows: the resident
+  // blocks sweep one narrow band of rows together, so the neighbour rows of
+  // the gathered vector p_{k-1} are still in L2 when they are needed again.
+  const int64_t stride = (int64_t)gridDim.x * rpp;
 
-  R ar[V], ai[V];
-  double w0[V], w1[V], w2[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    const int col = lane * V + v;
-    const bool neg = (a.c.neg_mask >> col) & 1ull;
-    const int set = (int)((a.c.set_mask >> col) & 1ull);
-    ar[v] = (R)(neg ? -a.c.alpha_re : a.c.alpha_re);
-    ai[v] = (R)(neg ? -a.c.alpha_im : a.c.alpha_im);
-    w0[v] = a.c.w[set][0];
-    w1[v] = a.c.w[set][1];
-    w2[v] = a.c.w[set][2];
-  }
+  // per-column selectors; the coefficients themselves stay in the parameter
+  // bank and are picked at their point of use (keeps registers free)
+  const unsigned neg_bits = (unsigned)(a.c.neg_mask >> (lane * V)) & ((1u << V) - 1u);
+  const unsigned set_bits = (unsigned)(a.c.set_mask >> (lane * V)) & ((1u << V) - 1u);
   const R beta = (R)a.c.beta;
-  const int nflush = a.c.nflush;
-  const bool do_corr = a.ref != nullptr;
-  const bool ref_lane = do_corr && lane < a.ref_tpr;
+  constexpr int BW = MODE == 0 ? TBPM_BW_PLAIN : TBPM_BW_FLUSH;
+  const int nflush = MODE >= 1 ? a.c.nflush : 0;
+  constexpr bool do_corr = MODE == 2;
+  const bool ref_lane = do_corr && a.ref != nullptr && lane < a.ref_tpr;
 
   double cre[V], cim[V], nrm[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) cre[v] = cim[v] = nrm[v] = 0.0;
 
-  for (int64_t r = r0 + slot; r < r1; r += rpp) {
+  for (int64_t r = (int64_t)blockIdx.x * rpp + slot; r < a.n_rows; r += stride) {
+    const int64_t e = r * tpr + lane;
+    // streamed operands first, so their latency overlaps the gather
+    Pack<R, V> pm2;
+    if (a.pin) {
+      pm2 = ldcs_pack(a.pin + e);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 2 * V; ++k) pm2.v[k] = (R)0;
+    }
     const int j0 = __ldg(a.indptr + r);
     const int j1 = __ldg(a.indptr + r + 1);
     R sre[V], sim[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) sre[v] = sim[v] = (R)0;
-    for (int j = j0; j < j1; ++j) {
-      const int c = __ldg(a.indices + j);
-      const typename Cx<R>::t h = ldg_c(a.hop + j);
-      const Pack<R, V> x = ldg_pack(a.gather + (int64_t)c * tpr + lane);
+    // neighbours in batches of BW independent gathers (graphene rows hold 3-4)
+    for (int jb = j0; jb < j1; jb += BW) {
+      int cidx[BW];
+      typename Cx<R>::t h[BW];
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        sre[v] = fma(h.x, x.v[2 * v], fma(-h.y, x.v[2 * v + 1], sre[v]));
-        sim[v] = fma(h.x, x.v[2 * v + 1], fma(h.y, x.v[2 * v], sim[v]));
+      for (int u = 0; u < BW; ++u) {
+        if (jb + u < j1) {
+          cidx[u] = __ldg(a.indices + jb + u);
+          h[u] = ldg_c(a.hop + jb + u);
+        } else {
+          cidx[u] = -1;
+        }
       }
-    }
-    const int64_t e = r * tpr + lane;
-    Pack<R, V> pm2;
-    if (a.pin) {
-      pm2 = a.pin[e];
-    } else {
+      Pack<R, V> x[BW];
 #pragma unroll
-      for (int k = 0; k < 2 * V; ++k) pm2.v[k] = (R)0;
+      for (int u = 0; u < BW; ++u)
+        if (cidx[u] >= 0) x[u] = ldg_pack(a.gather + (int64_t)cidx[u] * tpr + lane);
+#pragma unroll
+      for (int u = 0; u < BW; ++u) {
+        if (cidx[u] >= 0) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            sre[v] = fma(h[u].x, x[u].v[2 * v], fma(-h[u].y, x[u].v[2 * v + 1], sre[v]));
+            sim[v] = fma(h[u].x, x[u].v[2 * v + 1], fma(h[u].y, x[u].v[2 * v], sim[v]));
+          }
+        }
+      }
     }
     Pack<R, V> pk;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      pk.v[2 * v] = fma(ar[v], sre[v], fma(-ai[v], sim[v], beta * pm2.v[2 * v]));
-      pk.v[2 * v + 1] = fma(ar[v], sim[v], fma(ai[v], sre[v], beta * pm2.v[2 * v + 1]));
+      const bool neg = (neg_bits >> v) & 1u;
+      const R ar = (R)(neg ? -a.c.alpha_re : a.c.alpha_re);
+      const R ai = (R)(neg ? -a.c.alpha_im : a.c.alpha_im);
+      pk.v[2 * v] = fma(ar, sre[v], fma(-ai, sim[v], beta * pm2.v[2 * v]));
+      pk.v[2 * v + 1] = fma(ar, sim[v], fma(ai, sre[v], beta * pm2.v[2 * v + 1]));
     }
     if (nflush > 0) {
       Pack<R, V> pm1;
-      if (nflush >= 2) pm1 = a.gather[e];
+      if (nflush >= 2) pm1 = ldg_pack(a.gather + e);
       Pack<R, V> acc;
-      if (!a.c.acc_init) acc = a.acc[e];
+      if (!a.c.acc_init) acc = ldcs_pack(a.acc + e);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
+        const int set = (set_bits >> v) & 1u;
+        const double w0 = set ? a.c.w[1][0] : a.c.w[0][0];
+        const double w1 = set ? a.c.w[1][1] : a.c.w[0][1];
+        const double w2 = set ? a.c.w[1][2] : a.c.w[0][2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int k = 2 * v + q;
           double t = a.c.acc_init ? 0.0 : (double)acc.v[k];
-          if (nflush >= 3) t += w0[v] * (double)pm2.v[k];
-          if (nflush >= 2) t += w1[v] * (double)pm1.v[k];
-          t += w2[v] * (double)pk.v[k];
+          if (nflush >= 3) t += w0 * (double)pm2.v[k];
+          if (nflush >= 2) t += w1 * (double)pm1.v[k];
+          t += w2 * (double)pk.v[k];
           acc.v[k] = (R)t;
         }
       }
-      a.acc[e] = acc;
+      stcs_pack(a.acc + e, acc);
       if (do_corr) {
         Pack<R, V> rf;
-        if (ref_lane) rf = ldg_pack(a.ref + r * a.ref_tpr + lane);
+        if (ref_lane) rf = ldcs_pack(a.ref + r * a.ref_tpr + lane);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
           const double xr = (double)acc.v[2 * v], xi = (double)acc.v[2 * v + 1];
@@ -147,7 +187,7 @@ __global__ void __launch_bounds__(512) cheb_term_kernel(const TermArgs<R, V> a) 
         }
       }
     }
-    if (a.pout) a.pout[e] = pk;
+    if (a.pout) stcs_pack(a.pout + e, pk);
   }
 
   if (do_corr) {
@@ -212,13 +252,13 @@ __global__ void __launch_bounds__(512) corr_kernel(const Pack<R, V>* x, const Pa
   const int slot = threadIdx.x / tpr;
   const int lane = threadIdx.x - slot * tpr;
   const int rpp = blockDim.x / tpr;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
-  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
+  (void)rows_per_tile;  // grid-stride over row tiles of rpp rows
   const bool ref_lane = ref != nullptr && lane < ref_tpr;
   double cre[V], cim[V], nrm[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) cre[v] = cim[v] = nrm[v] = 0.0;
-  for (int64_t r = r0 + slot; r < r1; r += rpp) {
+  for (int64_t r = (int64_t)blockIdx.x * rpp + slot; r < n_rows;
+       r += (int64_t)gridDim.x * rpp) {
     const Pack<R, V> xv = ldg_pack(x + r * tpr + lane);
     Pack<R, V> rf;
     if (ref_lane) rf = ldg_pack(ref + r * ref_tpr + lane);
@@ -300,8 +340,7 @@ __global__ void __launch_bounds__(512) gen_state_kernel(StateKeys keys, int kind
   const int slot = threadIdx.x / tpr;
   const int lane = threadIdx.x - slot * tpr;
   const int rpp = blockDim.x / tpr;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
-  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
+  (void)rows_per_tile;  // grid-stride over row tiles of rpp rows
   const double two_pi = 6.283185307179586476925286766559;
   double acc[V];
   double den[V];
@@ -310,7 +349,8 @@ __global__ void __launch_bounds__(512) gen_state_kernel(StateKeys keys, int kind
     acc[v] = 0.0;
     den[v] = mode == 1 ? sqrt(sums[(int64_t)(lane * V + v) * sums_stride]) : 1.0;
   }
-  for (int64_t r = r0 + slot; r < r1; r += rpp) {
+  for (int64_t r = (int64_t)blockIdx.x * rpp + slot; r < n_rows;
+       r += (int64_t)gridDim.x * rpp) {
     Pack<R, V> o;
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -399,14 +439,14 @@ __global__ void __launch_bounds__(512) jcorr_kernel(
   const int slot = threadIdx.x / tpr;
   const int b = threadIdx.x - slot * tpr;
   const int rpp = blockDim.x / tpr;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
-  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
+  (void)rows_per_tile;  // grid-stride over row tiles of rpp rows
   const R s = (R)rescale;
   const int ld = 3 * B;
   double acc[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-  for (int64_t r = r0 + slot; r < r1; r += rpp) {
+  for (int64_t r = (int64_t)blockIdx.x * rpp + slot; r < n_rows;
+       r += (int64_t)gridDim.x * rpp) {
     R xxr = 0, xxi = 0, yxr = 0, yxi = 0, xyr = 0, xyi = 0, yyr = 0, yyi = 0;
     const int j0 = __ldg(indptr + r), j1 = __ldg(indptr + r + 1);
     for (int j = j0; j < j1; ++j) {

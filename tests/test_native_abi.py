@@ -1,0 +1,74 @@
+"""The C ABI library without a GPU: it loads, exports every function that
+include/tbpm_b200.h declares, computes host-only quantities, and refuses to
+run device work when no GPU is present (no CPU fallback)."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import tbplas_b200 as tb
+from tbplas_b200 import _native as nat
+from oracle import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "tbpm_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tbpm_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_function():
+    lib = nat.load_library()
+    declared = _declared_functions()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert sorted(nat.EXPORTED_SYMBOLS) == declared
+    assert lib.tbpm_version() == 1
+
+
+def test_fermi_coefficients_host_only_match_oracle():
+    beta = 9.0 / (tb.KB * 300)
+    for mu, omf in ((0.0, False), (0.0, True), (0.02, False)):
+        a = nat.fermi_cheb_coef(2**15, beta, mu, omf, 1e-12)
+        b = oracle.fermi_cheb_coef(2**15, beta, mu, omf, 1e-12)
+        assert a.size == b.size
+        assert np.max(np.abs(a - b)) < 1e-14
+    with pytest.raises(ValueError):
+        nat.fermi_cheb_coef(1000, beta, 0.0, False, 1e-12)  # not a power of two
+
+
+def _gpu_present():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_gpu_present(), reason="checks the behaviour without a GPU")
+def test_no_gpu_fails_loudly():
+    with pytest.raises(nat.TbpmError):
+        nat.Context(0)
+    from tbplas_b200.fortran import f2py
+    s = tb.make_graphene_sample(4, 4)
+    h = s.build_ham_csr()
+    nat._contexts.clear()
+    with pytest.raises(nat.TbpmError):
+        f2py.tbpm_dos([1.0, 0.1, 0.01], h.indptr, h.indices, h.data, 1, 4, 1, "", 0, 128, 1e-9)
+
+
+def test_f2py_argument_validation_happens_on_host():
+    from tbplas_b200.fortran import f2py
+    with pytest.raises(ValueError):
+        f2py._csr(np.array([0, 2 ** 40]), np.array([0]), np.array([1.0]))
+    with pytest.raises(ValueError):
+        f2py._csr(np.array([0]), np.array([]), np.array([]))
+    with pytest.raises(ValueError):
+        f2py.set_backend(precision="fp16")
+    with pytest.raises(ValueError):
+        f2py.set_backend(nonsense=1)
