@@ -43,6 +43,10 @@ DISORDER_W = 1.0
 RESCALE = 9.0
 SEED = 1337
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over the
+# algorithmic bytes of the same launches, measured on the 1024x1024 case
+# (profiles/cheb_term_kernel_fp64_graphene.md); traffic scales with the rows.
+TRAFFIC_OVER_ALGORITHMIC_FP64 = 0.982
 
 
 def log(*a):
@@ -313,7 +317,9 @@ def run_gpu(args):
                 "unit": "GB/s",
                 "frac": r64["achieved_gbs"] / peak,
                 "peak_kind": peak_kind,
-                "traffic": None,
+                "traffic": r64["alg_bytes_per_step"] * TRAFFIC_OVER_ALGORITHMIC_FP64,
+                "traffic_note": "bytes per step: ncu DRAM bytes / algorithmic bytes = 0.982 on "
+                                "the 1024x1024 case, scaled by rows to this workload",
                 "alg_bytes_per_step": r64["alg_bytes_per_step"],
                 "kernel": "cheb_term_kernel<double,1> (+ finalize_kernel, <1% of step)",
             },

@@ -120,6 +120,7 @@ int tbpm_destroy(tbpm_ctx* c) {
   c->ham.hop.release();
   c->ham.dx.release();
   c->ham.dy.release();
+  c->ham.diag.release();
   cudaStreamDestroy(c->stream);
   delete c;
   return TBPM_OK;
@@ -180,6 +181,8 @@ int tbpm_ham_release(tbpm_ctx* c) {
     c->ham.hop.release();
     c->ham.dx.release();
     c->ham.dy.release();
+    c->ham.diag.release();
+    c->ham.has_diag = false;
     c->ham.n = 0;
     c->ham.nnz = 0;
     c->ham.has_dxy = false;

@@ -40,11 +40,15 @@ struct DevMem {
   ~DevMem() { release(); }
 };
 
+// H = D + O: the diagonal D (on-site terms, dense complex[N]) and the
+// off-diagonal part O in CSR (indptr/indices/hop and the matching dx/dy).
+// nnz counts the entries of O.
 struct Ham {
   int prec = -1;
   int64_t n = 0, nnz = 0;
-  DevMem indptr, indices, hop, dx, dy;
+  DevMem indptr, indices, hop, dx, dy, diag;
   bool has_dxy = false;
+  bool has_diag = false;
   double rescale = 1.0;
 };
 

@@ -36,9 +36,10 @@ struct TermCoef {
 
 template <typename R, int V>
 struct TermArgs {
-  const int32_t* indptr;
+  const int32_t* indptr;   // off-diagonal CSR of H
   const int32_t* indices;
   const typename Cx<R>::t* hop;
+  const typename Cx<R>::t* diag;  // diagonal of H (null: none)
   int64_t n_rows;
   int64_t rows_per_tile;  // unused by the grid-stride kernels (kept for layout)
   int tpr;  // threads (packs) per row = ld / V
@@ -56,25 +57,54 @@ struct TermArgs {
 // 2 = flush + correlation/norm partials (last term of a time step).  Each
 // mode is compiled separately so the common mode-0 terms keep few registers.
 // Blocks have at most 256 threads; the minimum resident blocks per SM bound
-// the registers per thread (4 blocks: 64 registers, 5 blocks: 51).
-#ifndef TBPM_MINB_PLAIN
-#define TBPM_MINB_PLAIN 4
+// the registers per thread (4 blocks: 64 registers).
+// (measured on B200: FP64 is fastest at 4 resident blocks in every mode, the
+// FP32 recurrence-only mode at 5)
+#ifndef TBPM_MINB_PLAIN_F64
+#define TBPM_MINB_PLAIN_F64 4
+#endif
+#ifndef TBPM_MINB_PLAIN_F32
+#define TBPM_MINB_PLAIN_F32 5
 #endif
 #ifndef TBPM_MINB_FLUSH
 #define TBPM_MINB_FLUSH 4
 #endif
-// neighbours gathered per batch (independent loads in flight per thread)
-#ifndef TBPM_BW_PLAIN
-#define TBPM_BW_PLAIN 4
+
+template <typename R, int MODE>
+struct TermBounds {
+  static constexpr int min_blocks =
+      MODE == 0 ? (sizeof(R) == 8 ? TBPM_MINB_PLAIN_F64 : TBPM_MINB_PLAIN_F32) : TBPM_MINB_FLUSH;
+};
+// independent gathers issued per batch
+#ifndef TBPM_BW
+#define TBPM_BW 2
 #endif
-#ifndef TBPM_BW_FLUSH
-#define TBPM_BW_FLUSH 2
+// L2 prefetch distance in sweep iterations (0: off)
+#ifndef TBPM_PF_DIST
+#define TBPM_PF_DIST 1
 #endif
 
+// Bulk prefetch of [p, p + bytes) into L2 (sm_90+ cp.async.bulk.prefetch);
+// the range is trimmed to 16-byte granularity and to [lo, hi).
+__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes, const void* lo,
+                                            const void* hi) {
+  uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  uintptr_t e = a + (uintptr_t)bytes;
+  const uintptr_t l = reinterpret_cast<uintptr_t>(lo), h = reinterpret_cast<uintptr_t>(hi);
+  if (a < l) a = l;
+  if (e > h) e = h;
+  a = (a + 15) & ~(uintptr_t)15;
+  e = e & ~(uintptr_t)15;
+  if (e <= a) return;
+  const uint32_t sz = (uint32_t)(e - a);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(sz) : "memory");
+}
+
 template <typename R, int V, int MODE>
-__global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_FLUSH))
+__global__ void __launch_bounds__(256, (TermBounds<R, MODE>::min_blocks))
     cheb_term_kernel(const TermArgs<R, V> a) {
   extern __shared__ double smem[];
+  constexpr int BW = TBPM_BW;
   const int tpr = a.tpr;
   const int slot = threadIdx.x / tpr;
   const int lane = threadIdx.x - slot * tpr;
@@ -83,24 +113,44 @@ __global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_
   // blocks sweep one narrow band of rows together, so the neighbour rows of
   // the gathered vector p_{k-1} are still in L2 when they are needed again.
   const int64_t stride = (int64_t)gridDim.x * rpp;
-
   // per-column selectors; the coefficients themselves stay in the parameter
   // bank and are picked at their point of use (keeps registers free)
   const unsigned neg_bits = (unsigned)(a.c.neg_mask >> (lane * V)) & ((1u << V) - 1u);
   const unsigned set_bits = (unsigned)(a.c.set_mask >> (lane * V)) & ((1u << V) - 1u);
   const R beta = (R)a.c.beta;
-  constexpr int BW = MODE == 0 ? TBPM_BW_PLAIN : TBPM_BW_FLUSH;
   const int nflush = MODE >= 1 ? a.c.nflush : 0;
   constexpr bool do_corr = MODE == 2;
   const bool ref_lane = do_corr && a.ref != nullptr && lane < a.ref_tpr;
+  const bool need_own = a.diag != nullptr || nflush >= 2;
 
   double cre[V], cim[V], nrm[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) cre[v] = cim[v] = nrm[v] = 0.0;
 
-  for (int64_t r = (int64_t)blockIdx.x * rpp + slot; r < a.n_rows; r += stride) {
+  const int64_t row_bytes = (int64_t)tpr * sizeof(Pack<R, V>);
+  const char* gather_end = reinterpret_cast<const char*>(a.gather + a.n_rows * tpr);
+  for (int64_t r0 = (int64_t)blockIdx.x * rpp; r0 < a.n_rows; r0 += stride) {
+    if (TBPM_PF_DIST > 0 && threadIdx.x == 0) {
+      // the streamed tiles of this block TBPM_PF_DIST sweep iterations ahead:
+      // their DRAM reads are in flight without holding registers
+      const int64_t rp = r0 + TBPM_PF_DIST * stride;
+      if (rp < a.n_rows) {
+        const int64_t tile = (int64_t)rpp * row_bytes;
+        const char* g = reinterpret_cast<const char*>(a.gather);
+        prefetch_l2(g + rp * row_bytes, tile, g, gather_end);
+        if (a.pin) {
+          const char* p = reinterpret_cast<const char*>(a.pin);
+          prefetch_l2(p + rp * row_bytes, tile, p, p + a.n_rows * row_bytes);
+        }
+        if (MODE >= 1 && !a.c.acc_init) {
+          const char* q = reinterpret_cast<const char*>(a.acc);
+          prefetch_l2(q + rp * row_bytes, tile, q, q + a.n_rows * row_bytes);
+        }
+      }
+    }
+    const int64_t r = r0 + slot;
+    if (r >= a.n_rows) continue;
     const int64_t e = r * tpr + lane;
-    // streamed operands first, so their latency overlaps the gather
     Pack<R, V> pm2;
     if (a.pin) {
       pm2 = ldcs_pack(a.pin + e);
@@ -108,12 +158,23 @@ __global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_
 #pragma unroll
       for (int k = 0; k < 2 * V; ++k) pm2.v[k] = (R)0;
     }
+    Pack<R, V> own;
+    if (need_own) own = ldg_pack(a.gather + e);
     const int j0 = __ldg(a.indptr + r);
     const int j1 = __ldg(a.indptr + r + 1);
     R sre[V], sim[V];
+    if (a.diag) {
+      const typename Cx<R>::t d = ldg_c(a.diag + r);
 #pragma unroll
-    for (int v = 0; v < V; ++v) sre[v] = sim[v] = (R)0;
-    // neighbours in batches of BW independent gathers (graphene rows hold 3-4)
+      for (int v = 0; v < V; ++v) {
+        sre[v] = d.x * own.v[2 * v] - d.y * own.v[2 * v + 1];
+        sim[v] = d.x * own.v[2 * v + 1] + d.y * own.v[2 * v];
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) sre[v] = sim[v] = (R)0;
+    }
+    // off-diagonal neighbours in batches of BW independent gathers
     for (int jb = j0; jb < j1; jb += BW) {
       int cidx[BW];
       typename Cx<R>::t h[BW];
@@ -151,8 +212,6 @@ __global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_
       pk.v[2 * v + 1] = fma(ar, sim[v], fma(ai, sre[v], beta * pm2.v[2 * v + 1]));
     }
     if (nflush > 0) {
-      Pack<R, V> pm1;
-      if (nflush >= 2) pm1 = ldg_pack(a.gather + e);
       Pack<R, V> acc;
       if (!a.c.acc_init) acc = ldcs_pack(a.acc + e);
 #pragma unroll
@@ -166,7 +225,7 @@ __global__ void __launch_bounds__(256, (MODE == 0 ? TBPM_MINB_PLAIN : TBPM_MINB_
           const int k = 2 * v + q;
           double t = a.c.acc_init ? 0.0 : (double)acc.v[k];
           if (nflush >= 3) t += w0 * (double)pm2.v[k];
-          if (nflush >= 2) t += w1 * (double)pm1.v[k];
+          if (nflush >= 2) t += w1 * (double)own.v[k];
           t += w2 * (double)pk.v[k];
           acc.v[k] = (R)t;
         }
