@@ -187,6 +187,25 @@ int tbpm_cheb_timestep(tbpm_ctx* ctx, const double* bes, int n_bes, double* wf,
 int tbpm_fermi_apply(tbpm_ctx* ctx, const double* coef, int n_coef, double* wf,
                      int n_states);
 
+/* One time step psi <- exp(-/+ i H dt) psi that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc (or have the library call it), e.g. a framework whose caching
+ * allocator owns nearly all of HBM, or a loop where allocation after start-up
+ * is forbidden.  All array arguments except bes are DEVICE pointers from the
+ * caller's own allocator: the full CSR (diagonal entries included) and
+ * wf = complex128 [n_rows][n_states] row-interleaved, updated in place.  The
+ * two work vectors come from a fixed 16 MiB array inside the library (held by
+ * every GPU that loads it until exit), so n_rows * n_states may be at most
+ * 524,272; larger sizes return TBPM_ERR_ARG.  The first call on a device looks
+ * up that array's device address (make it before any stream capture).  All
+ * calls share the array: calls that overlap on the GPU race, so serialise
+ * them.  The call validates the CSR on the device and is synchronous on the
+ * context stream.  FP64 only. */
+int tbpm_cheb_timestep_noalloc(tbpm_ctx* ctx, const double* bes, int n_bes,
+                               const int32_t* indptr, const int32_t* indices,
+                               const double* hop, int64_t n_rows, int64_t nnz, double* wf,
+                               int n_states, int forward);
+
 /* ---- device-resident propagation session (benchmarks, batching) --------- */
 
 /* Start a DOS propagation of n_states random states (seed rule as

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "tbpm_accond", "tbpm_accond_states", "tbpm_dccond", "tbpm_dccond_states",
     "tbpm_psi_t", "tbpm_random_states", "tbpm_fermi_cheb_coef",
     "tbpm_cheb_timestep", "tbpm_fermi_apply", "tbpm_session_dos_begin",
-    "tbpm_session_advance", "tbpm_session_read",
+    "tbpm_session_advance", "tbpm_session_read", "tbpm_cheb_timestep_noalloc",
 )
 
 
@@ -111,6 +111,8 @@ _SIGNATURES = {
                                         _c_int]),
     "tbpm_session_advance": (_c_int, [_vp, _c_int]),
     "tbpm_session_read": (_c_int, [_vp, _vp, _vp, ctypes.POINTER(_c_int)]),
+    "tbpm_cheb_timestep_noalloc": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64,
+                                            _vp, _c_int, _c_int]),
 }
 
 _lib = None

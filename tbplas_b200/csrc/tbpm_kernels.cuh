@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256, (TermBounds<R, MODE>::min_blocks))
 
 // Sum block partials laid out as [value][n_blocks] into out[step][value];
 // block b handles value b.  The last block to finish advances *step.
-__global__ void __launch_bounds__(256) finalize_kernel(const double* partials, int n_blocks,
+static __global__ void __launch_bounds__(256) finalize_kernel(const double* partials, int n_blocks,
                                                        int n_values, int* step,
                                                        unsigned int* done, double* out) {
   __shared__ double red[256];
