@@ -63,6 +63,8 @@ typedef struct tbpm_options {
   int use_graphs;        /* 1 (default): replay captured CUDA graphs */
   double fp32_chk_thr;   /* lower bound of the norm-check threshold in FP32
                             mode (default 1e-4); FP64 uses wfn_chk_thr as is */
+  int vector_width;      /* complex values per thread and load in FP32 mode:
+                            0 = automatic (2 when the block width allows), 1, 2 */
 } tbpm_options;
 
 /* ---- context ------------------------------------------------------------ */
@@ -75,8 +77,9 @@ int tbpm_set_options(tbpm_ctx* ctx, const tbpm_options* opts);
 int tbpm_get_options(const tbpm_ctx* ctx, tbpm_options* opts);
 /* The cudaStream_t (as void*) all work of the context is enqueued on. */
 void* tbpm_get_stream(const tbpm_ctx* ctx);
-/* Statistics of the last propagation: kernel launches enqueued and the model
- * of algorithmic HBM bytes they move (see DESIGN.md of the source tree). */
+/* Statistics of the last propagation: kernel launches enqueued and the
+ * algorithmic HBM bytes they move (CSR and every vector pass of the fused
+ * schedule counted once; neighbour re-reads assumed to hit L2). */
 int tbpm_last_stats(const tbpm_ctx* ctx, int64_t* kernel_launches, double* model_bytes);
 int tbpm_version(void);
 
@@ -159,6 +162,22 @@ int tbpm_psi_t(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indpt
                const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
                const double* psi0, const int32_t* time_log, int n_time_log, int n_timestep,
                int wfn_chk_step, double wfn_chk_thr, double* psi_t);
+
+/* DOS correlations of many uneven realisations packed into one block-diagonal
+ * Hamiltonian (a batch of samples; the TBPM loop of tbpm.f90:50-86 run for
+ * every realisation at once).  Realisation k owns rows
+ * [seg_offsets[k], seg_offsets[k+1]) (seg_offsets[0] = 0,
+ * seg_offsets[n_seg] = n_rows) and n_states random states drawn over its own
+ * rows with iseed = seed*(k*n_states + s + 1) and normalised there.  All
+ * realisations share the Bessel series (one rescale factor).  The whole
+ * propagation is captured as one CUDA graph and launched once.
+ * corr: complex128 [n_seg][n_timestep+1] (state average per realisation);
+ * corr_per_state (optional): complex128 [n_seg][n_states][n_timestep+1]. */
+int tbpm_dos_segmented(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+                       const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+                       const int64_t* seg_offsets, int n_seg, int n_states, int seed,
+                       int n_timestep, int wfn_chk_step, double wfn_chk_thr, double* corr,
+                       double* corr_per_state);
 
 /* ---- building blocks ----------------------------------------------------- */
 

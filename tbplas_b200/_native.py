@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "tbpm_psi_t", "tbpm_random_states", "tbpm_fermi_cheb_coef",
     "tbpm_cheb_timestep", "tbpm_fermi_apply", "tbpm_session_dos_begin",
     "tbpm_session_advance", "tbpm_session_read", "tbpm_cheb_timestep_noalloc",
+    "tbpm_dos_segmented",
 )
 
 
@@ -64,6 +65,7 @@ class Options(ctypes.Structure):
         ("steps_per_graph", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
         ("fp32_chk_thr", ctypes.c_double),
+        ("vector_width", ctypes.c_int),
     ]
 
 
@@ -113,6 +115,8 @@ _SIGNATURES = {
     "tbpm_session_read": (_c_int, [_vp, _vp, _vp, ctypes.POINTER(_c_int)]),
     "tbpm_cheb_timestep_noalloc": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64,
                                             _vp, _c_int, _c_int]),
+    "tbpm_dos_segmented": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64, _vp,
+                                    _c_int, _c_int, _c_int, _c_int, _c_int, _c_dbl, _vp, _vp]),
 }
 
 _lib = None

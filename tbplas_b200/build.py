@@ -19,7 +19,8 @@ INCLUDE = os.path.join(ROOT_DIR, "include")
 LIB_PATH = os.path.join(PKG_DIR, "libtbpm_b200.so")
 
 SOURCES = ["tbpm_engine.cu", "tbpm_capi.cu", "tbpm_noalloc.cu"]
-HEADERS = ["tbpm_common.cuh", "tbpm_kernels.cuh", "tbpm_dc_kernels.cuh", "tbpm_engine.cuh"]
+HEADERS = ["tbpm_common.cuh", "tbpm_kernels.cuh", "tbpm_dc_kernels.cuh", "tbpm_seg_kernels.cuh",
+           "tbpm_engine.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -34,6 +34,9 @@ void drv_fermi_coef(int nr_fermi, double beta, double mu, int one_minus, double 
 void drv_expansion_apply(tbpm_ctx* c, const Expansion& ex, double* wf, int n_states);
 void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_states, int seed,
                            int rank, int n_ran_samples, int n_timestep);
+void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t* seg_off,
+                       int n_seg, int n_states, int seed, int n_timestep, int chk_step,
+                       double chk_thr, double* corr, double* corr_per_state);
 void drv_session_advance(tbpm_ctx* c, int n_steps);
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done);
 }  // namespace tbpm
@@ -51,6 +54,7 @@ tbpm_options default_options() {
   o.steps_per_graph = 16;
   o.use_graphs = 1;
   o.fp32_chk_thr = 1e-4;
+  o.vector_width = 0;
   return o;
 }
 
@@ -139,7 +143,8 @@ int tbpm_set_options(tbpm_ctx* c, const tbpm_options* o) {
     return TBPM_ERR_ARG;
   }
   if (o->batch < 0 || o->threads_per_block < 0 || o->rows_per_tile < 0 ||
-      o->steps_per_graph < 0 || !(o->fp32_chk_thr >= 0)) {
+      o->steps_per_graph < 0 || !(o->fp32_chk_thr >= 0) || o->vector_width < 0 ||
+      o->vector_width > 2) {
     c->err = "negative option";
     return TBPM_ERR_ARG;
   }
@@ -321,6 +326,18 @@ int tbpm_fermi_apply(tbpm_ctx* c, const double* coef, int n_coef, double* wf, in
     if (!coef || n_coef < 3 || !wf) throw tbpm::Error{TBPM_ERR_ARG, "bad arguments"};
     const tbpm::Expansion ex = tbpm::fermi_expansion(coef, n_coef, coef, n_coef, 0ull);
     tbpm::drv_expansion_apply(c, ex, wf, n_states);
+  });
+}
+
+int tbpm_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int32_t* indptr,
+                       const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+                       const int64_t* seg_offsets, int n_seg, int n_states, int seed,
+                       int n_timestep, int wfn_chk_step, double wfn_chk_thr, double* corr,
+                       double* corr_per_state) {
+  return guarded(c, [&] {
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, nullptr, nullptr, 1.0);
+    tbpm::drv_dos_segmented(c, bes, n_bes, seg_offsets, n_seg, n_states, seed, n_timestep,
+                            wfn_chk_step, wfn_chk_thr, corr, corr_per_state);
   });
 }
 

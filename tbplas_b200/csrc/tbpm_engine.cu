@@ -20,6 +20,7 @@
 
 #include "tbpm_engine.cuh"
 #include "tbpm_dc_kernels.cuh"
+#include "tbpm_seg_kernels.cuh"
 #include "tbpm_kernels.cuh"
 
 namespace tbpm {
@@ -434,9 +435,11 @@ StateKeys make_keys(int seed, int first_sample, int n_states, int rank, int n_ra
   return k;
 }
 
-int pick_V(int prec, int ld, int group) {
+int pick_V(int prec, int ld, int group, int requested = 0) {
   if (prec == TBPM_PREC_FP64) return 1;
-  return (ld % 2 == 0 && group % 2 == 0) ? 2 : 1;
+  const bool can2 = ld % 2 == 0 && group % 2 == 0;
+  if (requested == 1) return 1;
+  return can2 ? 2 : 1;
 }
 
 void require_ham(const tbpm_ctx* c, bool need_dxy) {
@@ -456,10 +459,15 @@ int batch_size(const tbpm_ctx* c) {
 
 // ---- CUDA graph replay of a per-step program ---------------------------------
 
+// Enqueue n_steps of `step`: replay a CUDA graph of G captured steps as often
+// as it fits (G = graph_steps if positive, else opts.steps_per_graph), the
+// remainder directly.
 template <class Fn>
-void run_steps(tbpm_ctx* c, int n_steps, const std::vector<unsigned char>& key, Fn&& step) {
+void run_steps(tbpm_ctx* c, int n_steps, const std::vector<unsigned char>& key, Fn&& step,
+               int graph_steps = 0) {
   if (n_steps <= 0) return;
-  const int G = c->opts.steps_per_graph > 0 ? c->opts.steps_per_graph : 16;
+  const int G = graph_steps > 0 ? graph_steps
+                                : (c->opts.steps_per_graph > 0 ? c->opts.steps_per_graph : 16);
   int done = 0;
   if (c->opts.use_graphs && n_steps >= G) {
     if (!c->graph.exec || c->graph.key != key || c->graph.steps != G) {
@@ -671,6 +679,108 @@ void dos_batch(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys* keys,
     }
   }
   (void)total_states;
+}
+
+
+// ---- batches of uneven realisations (block-diagonal packing) -----------------
+
+// One DOS propagation of n_seg packed realisations x ns states each.  corr:
+// complex [n_seg][n_timestep+1], averaged over the ns states of a realisation;
+// corr_per_state (optional): complex [n_seg][ns][n_timestep+1].  The whole
+// propagation is captured as a single CUDA graph and launched once.
+template <typename R>
+void dos_segmented_run(tbpm_ctx* c, const Expansion& ex, const std::vector<int64_t>& off,
+                       int ns, int seed, int n_timestep, int chk_step, double chk_thr,
+                       double* corr, double* corr_per_state) {
+  constexpr int V = 1;
+  using C = typename Cx<R>::t;
+  const int n_seg = (int)off.size() - 1;
+  const int64_t n = c->ham.n;
+  int64_t max_len = 0;
+  for (int k = 0; k < n_seg; ++k) max_len = std::max<int64_t>(max_len, off[k + 1] - off[k]);
+  const int64_t rows_per_chunk = 4096;
+  const int n_chunks = (int)std::max<int64_t>(1, (max_len + rows_per_chunk - 1) / rows_per_chunk);
+  const int rpp = std::max(1, 256 / ns);
+  const int threads = rpp * ns;
+  const int n_values = n_seg * ns * 3;
+  c->graph.reset();
+  c->sess.active = false;
+  ensure_vectors(c, ns, ns);
+  c->seg.ensure(sizeof(int64_t) * off.size());
+  TBPM_CK(cudaMemcpyAsync(c->seg.p, off.data(), sizeof(int64_t) * off.size(),
+                          cudaMemcpyHostToDevice, c->stream));
+  ensure_partials(c, (size_t)n_values * n_chunks);
+  c->small.ensure(sizeof(double) * std::max<size_t>((size_t)n_seg * ns, kMaxCols * 2));
+  c->out.ensure((size_t)(n_timestep + 1) * n_values * sizeof(double));
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  const dim3 grid(n_chunks, n_seg);
+  // random states, normalised per realisation
+  reset_counters(c, 1);
+  seg_state_kernel<R><<<grid, threads, 0, c->stream>>>(
+      c->seg.as<int64_t>(), ns, (long long)seed, c->opts.state_kind, rows_per_chunk, 0, nullptr,
+      nullptr, c->partials.as<double>());
+  TBPM_CK(cudaGetLastError());
+  launch_finalize(c, n_chunks, n_seg * ns, counters(c, 1), c->small.as<double>());
+  seg_state_kernel<R><<<grid, threads, 0, c->stream>>>(
+      c->seg.as<int64_t>(), ns, (long long)seed, c->opts.state_kind, rows_per_chunk, 1,
+      c->small.as<double>(), reinterpret_cast<C*>(W), nullptr);
+  TBPM_CK(cudaGetLastError());
+  c->launches += 2;
+  TBPM_CK(cudaMemcpyAsync(A, W, (size_t)n * ns * sizeof(C), cudaMemcpyDeviceToDevice, c->stream));
+  reset_counters(c, 0);
+  auto seg_corr = [&]() {
+    seg_corr_kernel<R><<<grid, threads, 0, c->stream>>>(
+        c->seg.as<int64_t>(), ns, rows_per_chunk, reinterpret_cast<const C*>(A),
+        reinterpret_cast<const C*>(W), c->partials.as<double>());
+    TBPM_CK(cudaGetLastError());
+    c->launches++;
+    c->model_bytes += 2.0 * (double)n * ns * sizeof(C);
+    launch_finalize(c, n_chunks, n_values, counters(c, 0), c->out.as<double>());
+  };
+  seg_corr();  // row 0: <wf0|wf0>
+  auto step = [&]() {
+    enqueue_expansion<R, V>(c, ex, ns, A, X, Y, nullptr, 0, nullptr, Counters{});
+    seg_corr();
+  };
+  std::vector<unsigned char> key = plan_key(c, 4, ns, V, ex);
+  key_push(key, n_seg);
+  const double thr = effective_thr(c, chk_thr);
+  std::vector<double> host;
+  int done = 0;
+  const bool check = chk_step >= 2 && chk_step <= n_timestep;
+  if (check) {
+    run_steps(c, chk_step - 1, key, step, chk_step - 1);
+    done = chk_step - 1;
+    read_out(c, host, (size_t)(done + 1) * n_values);
+    for (int v = 0; v < n_seg * ns; ++v) {
+      const double ref = host[((size_t)1 * n_seg * ns + v) * 3 + 2];
+      const double nv = host[((size_t)done * n_seg * ns + v) * 3 + 2];
+      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dos_segmented", chk_step);
+    }
+    c->graph.reset();
+  }
+  run_steps(c, n_timestep - done, key, step, n_timestep - done);
+  read_out(c, host, (size_t)(n_timestep + 1) * n_values);
+  c->graph.reset();
+  for (int k = 0; k < n_seg; ++k)
+    for (int t = 0; t <= n_timestep; ++t) {
+      double re = 0, im = 0;
+      for (int b = 0; b < ns; ++b) {
+        const double* v = &host[(((size_t)t * n_seg + k) * ns + b) * 3];
+        re += v[0] / ns;
+        im += v[1] / ns;
+        if (corr_per_state) {
+          double* o = corr_per_state + 2 * (((size_t)k * ns + b) * (n_timestep + 1) + t);
+          o[0] = v[0];
+          o[1] = v[1];
+        }
+      }
+      corr[2 * ((size_t)k * (n_timestep + 1) + t)] = re;
+      corr[2 * ((size_t)k * (n_timestep + 1) + t) + 1] = im;
+    }
 }
 
 // ---- AC ---------------------------------------------------------------------
@@ -1192,7 +1302,7 @@ void drv_dos(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n
       kp = &keys;
     }
     const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
-    dispatch(c->ham.prec, pick_V(c->ham.prec, ns, ns), [&](auto tag) {
+    dispatch(c->ham.prec, pick_V(c->ham.prec, ns, ns, c->opts.vector_width), [&](auto tag) {
       using P = decltype(tag);
       dos_batch<typename P::Real, P::V>(c, ex, ns, kp, hw, n_timestep, chk_step, chk_thr,
                                         n_states, corr, corr_per_state, s0, n_states);
@@ -1229,7 +1339,7 @@ void drv_ac(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
       kp = &keys;
     }
     const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
-    dispatch(c->ham.prec, pick_V(c->ham.prec, 3 * nb, nb), [&](auto tag) {
+    dispatch(c->ham.prec, pick_V(c->ham.prec, 3 * nb, nb, c->opts.vector_width), [&](auto tag) {
       using P = decltype(tag);
       ac_batch<typename P::Real, P::V>(c, ex_time, ex_fermi, nb, kp, hw, n_timestep, chk_step,
                                        chk_thr, n_states, corr);
@@ -1283,13 +1393,38 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
       kp = &keys;
     }
     const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
-    dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb), [&](auto tag) {
+    dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb, c->opts.vector_width), [&](auto tag) {
       using P = decltype(tag);
       dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep, t_step, en_sel,
                                        chk_step, chk_thr, n_states, n_energies, dos_corr,
                                        dc_corr);
     });
   }
+}
+
+void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t* seg_off,
+                       int n_seg, int n_states, int seed, int n_timestep, int chk_step,
+                       double chk_thr, double* corr, double* corr_per_state) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
+  if (!seg_off || n_seg < 1 || n_seg > 65535) throw Error{TBPM_ERR_ARG, "1..65535 segments"};
+  if (!corr) throw Error{TBPM_ERR_ARG, "null output"};
+  std::vector<int64_t> off(seg_off, seg_off + n_seg + 1);
+  if (off[0] != 0 || off[n_seg] != c->ham.n)
+    throw Error{TBPM_ERR_ARG, "segment offsets must start at 0 and end at n_rows"};
+  for (int k = 0; k < n_seg; ++k)
+    if (off[k + 1] < off[k]) throw Error{TBPM_ERR_ARG, "segment offsets must not decrease"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  const Expansion ex = time_step_expansion(bes, n_bes);
+  if (c->ham.prec == TBPM_PREC_FP64)
+    dos_segmented_run<double>(c, ex, off, n_states, seed, n_timestep, chk_step, chk_thr, corr,
+                              corr_per_state);
+  else
+    dos_segmented_run<float>(c, ex, off, n_states, seed, n_timestep, chk_step, chk_thr, corr,
+                             corr_per_state);
 }
 
 void drv_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const double* psi0,
@@ -1356,7 +1491,7 @@ void drv_expansion_apply(tbpm_ctx* c, const Expansion& ex, double* wf, int n_sta
   c->graph.reset();
   const int ld = n_states;
   ensure_vectors(c, ld, 1);
-  dispatch(c->ham.prec, pick_V(c->ham.prec, ld, ld), [&](auto tag) {
+  dispatch(c->ham.prec, pick_V(c->ham.prec, ld, ld, c->opts.vector_width), [&](auto tag) {
     using P = decltype(tag);
     using R = typename P::Real;
     constexpr int V = P::V;
@@ -1376,7 +1511,7 @@ void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_stat
   c->model_bytes = 0;
   const Expansion ex = time_step_expansion(bes, n_bes);
   const StateKeys keys = make_keys(seed, 1, n_states, rank, n_ran_samples);
-  dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states), [&](auto tag) {
+  dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states, c->opts.vector_width), [&](auto tag) {
     using P = decltype(tag);
     dos_session_begin<typename P::Real, P::V>(c, ex, n_states, &keys, nullptr, n_timestep + 1);
   });

@@ -100,7 +100,7 @@ struct tbpm_ctx {
   tbpm_options opts{};
   std::string err;
   tbpm::Ham ham;
-  tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef;
+  tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef, seg;
   int64_t launches = 0;
   double model_bytes = 0;
   tbpm::Session sess;

@@ -19,7 +19,7 @@ from .. import _native as nat
 
 __all__ = ["tbpm_dos", "tbpm_accond", "tbpm_dccond", "tbpm_psi_t", "tbpm_ldos",
            "tbpm_dos_states", "tbpm_accond_states", "tbpm_dccond_states",
-           "set_backend", "get_backend"]
+           "tbpm_dos_segmented", "set_backend", "get_backend"]
 
 _INT32_MAX = np.iinfo(np.int32).max
 
@@ -33,6 +33,7 @@ _backend = {
     "steps_per_graph": 16,
     "use_graphs": True,
     "fp32_chk_thr": 1.0e-4,
+    "vector_width": 0,       # FP32 complex values per thread: 0 auto, 1, 2
     "verbose": False,
 }
 
@@ -65,6 +66,7 @@ def _ctx() -> nat.Context:
         steps_per_graph=int(_backend["steps_per_graph"]),
         use_graphs=1 if _backend["use_graphs"] else 0,
         fp32_chk_thr=float(_backend["fp32_chk_thr"]),
+        vector_width=int(_backend["vector_width"]),
     )
     return ctx
 
@@ -283,3 +285,26 @@ def random_states(n_orbitals: int, seed: int, n_states: int, rank: int = 0,
                 int(n_states), int(rank), nrs,
                 nat.STATE_EXP if k == "exp" else nat.STATE_UNIT, nat.ptr(out))
     return out
+
+
+def tbpm_dos_segmented(bes, indptr, indices, hop, seg_offsets, n_states, seed, n_timestep,
+                       wfn_chk_step=128, wfn_chk_thr=1.0e-9, per_state: bool = False):
+    """DOS correlations of a batch of realisations packed block-diagonally
+    (tbplas_b200.builder.pack_samples), propagated together.
+
+    :param seg_offsets: (n_seg+1,) row offsets of the realisations
+    :return: (n_seg, n_timestep+1) complex128, the state average per
+        realisation; with per_state=True also (n_seg, n_states, n_timestep+1)
+    """
+    bes = nat.as_c(bes, np.float64)
+    ip, ix, hv, n, nnz = _csr(indptr, indices, hop)
+    off = nat.as_c(seg_offsets, np.int64)
+    n_seg = off.size - 1
+    corr = np.zeros((n_seg, int(n_timestep) + 1), dtype=np.complex128)
+    per = (np.zeros((n_seg, int(n_states), int(n_timestep) + 1), dtype=np.complex128)
+           if per_state else None)
+    _ctx().call("tbpm_dos_segmented", nat.ptr(bes), bes.size, nat.ptr(ip), nat.ptr(ix),
+                nat.ptr(hv), n, nnz, nat.ptr(off), n_seg, int(n_states), int(seed),
+                int(n_timestep), int(wfn_chk_step), float(wfn_chk_thr), nat.ptr(corr),
+                nat.ptr(per))
+    return (corr, per) if per_state else corr

@@ -21,6 +21,7 @@ seeded synthetic Hamiltonians and seeded Philox states.
 import argparse
 import json
 import math
+import os
 import sys
 import time
 
@@ -109,7 +110,69 @@ def run_c2(steps_dos: int = 1024, steps_ac: int = 1024, n_states: int = 16) -> d
     return res
 
 
-RUNNERS = {"c1": run_c1, "c2": run_c2}
+def _c3_sample(args):
+    nx, ny, w, seed = args
+    s = make_graphene_sample(nx, ny, disorder=w, vacancy_rate=0.01, rescale=10.0, seed=seed)
+    h = s.build_ham_csr()
+    return h.indptr.astype(np.int64), h.indices.astype(np.int32), h.data
+
+
+def build_c3(n_real: int = 64, lo: int = 256, hi: int = 1024, seed: int = 1337, workers=None):
+    """64 realisations with L_a, L_b ~ U{lo..hi} cells, W ~ U[0,3] eV, 1%
+    vacancies, rescale 10 eV (max row sum 3*2.7 + 1.5 < 10), packed
+    block-diagonally.  Built in a spawn-started process pool (host work only,
+    before any CUDA use in the workers)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(lo, hi + 1)), int(rng.integers(lo, hi + 1)),
+              float(rng.uniform(0, 3)), seed + 1 + i) for i in range(n_real)]
+    workers = workers or min(8, os.cpu_count() or 1)
+    with cf.ProcessPoolExecutor(max_workers=workers,
+                                mp_context=mp.get_context("spawn")) as ex:
+        parts = list(ex.map(_c3_sample, specs))
+    offsets = [0]
+    ips, ixs, vals = [], [], []
+    nnz = 0
+    for ip, ix, v in parts:
+        ips.append(ip[:-1] + nnz)
+        ixs.append(ix + offsets[-1])
+        vals.append(v)
+        nnz += v.size
+        offsets.append(offsets[-1] + ip.size - 1)
+    indptr = np.concatenate(ips + [np.array([nnz])]).astype(np.int32)
+    return (indptr, np.concatenate(ixs).astype(np.int32), np.concatenate(vals),
+            np.array(offsets, dtype=np.int64), specs)
+
+
+def run_c3(steps: int = 512, n_states: int = 4, n_real: int = 64, lo: int = 256,
+           hi: int = 1024) -> dict:
+    from . import autotune
+    (ip, ix, hv, off, specs), t_build = _timed(lambda: build_c3(n_real, lo, hi))
+    n = ip.size - 1
+    bes = bessel_series(math.pi)  # dt*rescale = 2*pi/(2*rescale)*rescale
+    res = {"workload": f"c3 {n_real} graphene realisations {lo}^2..{hi}^2, 1% vacancies, "
+                       f"W~U[0,3] eV, rescale 10, {n_states} states each, packed, one graph",
+           "n_orbitals_total": int(n), "nnz": int(hv.size), "steps": steps,
+           "host_build_seconds": t_build}
+    out = {}
+    for prec in ("fp64", "fp32"):
+        tuned = autotune.tune_dos(ip, ix, hv, n_states, prec, steps=2, bessel=bes)
+        autotune.apply(tuned["best"])
+        f2py.set_backend(precision=prec)
+        corr, sec = _timed(lambda: f2py.tbpm_dos_segmented(bes, ip, ix, hv, off, n_states,
+                                                           1337, steps))
+        res[f"{prec}_tuned"] = tuned["best"]
+        res[f"{prec}_seconds"] = sec
+        res[f"{prec}_orbital_steps_per_s"] = n * n_states * steps / sec
+        out[prec] = corr
+    diff = np.abs(out["fp32"] - out["fp64"]).max(axis=1) / np.abs(out["fp64"]).max(axis=1)
+    res["fp32_max_rel_corr_err_per_realisation"] = float(diff.max())
+    f2py.set_backend(precision="fp64", threads_per_block=0, vector_width=0)
+    return res
+
+
+RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3}
 
 
 def main(argv=None) -> None:
@@ -122,7 +185,7 @@ def main(argv=None) -> None:
     for w in args.workloads:
         kw = {}
         if args.steps:
-            kw = {"steps": args.steps} if w == "c1" else \
+            kw = {"steps": args.steps} if w in ("c1", "c3") else \
                  {"steps_dos": args.steps, "steps_ac": args.steps}
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
