@@ -1375,9 +1375,14 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
   {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && n_en_inds > 0) {
-      const size_t per_state = (size_t)c->ham.n * n_en_inds * 2 * real_size(c->ham.prec);
-      const size_t budget = free_b > ((size_t)4 << 30) ? free_b - ((size_t)4 << 30) : free_b / 2;
-      const int fit = (int)std::max<size_t>(1, budget / std::max<size_t>(per_state, 1) / 2);
+      // per state: its QE block (N x n_en complex) plus its two columns in
+      // the window ring (kMaxWindow + 1 slots) and in X, Y, wf0
+      const size_t cx = 2 * real_size(c->ham.prec);
+      const size_t per_state =
+          (size_t)c->ham.n * ((size_t)n_en_inds * cx + (size_t)(kMaxWindow + 4) * 2 * cx);
+      const size_t reserve = (size_t)6 << 30;
+      const size_t budget = free_b > 2 * reserve ? free_b - reserve : free_b / 2;
+      const int fit = (int)std::max<size_t>(1, budget / std::max<size_t>(per_state, 1));
       B = std::min(B, fit);
     }
     (void)cudaGetLastError();

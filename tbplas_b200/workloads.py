@@ -172,7 +172,55 @@ def run_c3(steps: int = 512, n_states: int = 4, n_real: int = 64, lo: int = 256,
     return res
 
 
-RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3}
+def run_c5(steps: int = 2048, n_states: int = 8, nx: int = 4096, precision: str = "fp32",
+           energy_limits=(-0.5, 0.5)) -> dict:
+    """DC conductivity of 4096x4096 graphene in a perpendicular field of one
+    flux quantum per 1024 hexagons (B = h/e / (1024 * hexagon area) = 77.06 T,
+    Peierls phases in the gauge A = (By, 0, 0)), Anderson W = 1 eV, through the
+    drop-in Solver / Analyzer."""
+    import tempfile
+    t0 = time.perf_counter()
+    s = make_graphene_sample(nx, nx, disorder=1.0, rescale=9.0, seed=1337)
+    flux_quantum = 4135.667  # h/e in T nm^2
+    b_field = flux_quantum / (1024 * s.area_unit_cell)
+    s.set_magnetic_field(b_field, gauge=0)
+    ham = s.build_ham_dxy()
+    t_build = time.perf_counter() - t0
+
+    class Prebuilt:  # the Sample interface with the arrays built once
+        rescale = s.rescale
+        energy_range = s.energy_range
+        nr_orbitals = s.nr_orbitals
+        area_unit_cell = s.area_unit_cell
+        volume_unit_cell = s.volume_unit_cell
+        extended = s.extended
+
+        def build_ham_dxy(self):
+            return ham
+
+    cfg = Config()
+    cfg.generic["nr_time_steps"] = steps
+    cfg.generic["nr_random_samples"] = n_states
+    cfg.DC_conductivity["energy_limits"] = energy_limits
+    with tempfile.TemporaryDirectory() as d:
+        solver = Solver(Prebuilt(), cfg, echo_details=False, directory=d, prefix="c5",
+                        backend={"precision": precision, "batch": n_states})
+        (corr_dos, corr_dc), sec = _timed(solver.calc_corr_dc_cond)
+    an = Analyzer(Prebuilt(), cfg, dimension=2)
+    energies, dc = an.calc_dc_cond(corr_dos, corr_dc)
+    i0 = int(np.argmin(np.abs(energies)))
+    n = ham[0].size - 1
+    f2py.set_backend(precision="fp64", batch=16)
+    return {"workload": f"c5 graphene {nx}x{nx}, B={b_field:.2f} T (flux h/e per 1024 "
+                        f"hexagons), W=1 eV, {n_states} states, corr_dc {precision}",
+            "n_orbitals": int(n), "steps": steps, "n_energies": int(energies.size),
+            "host_build_seconds": t_build, "seconds": sec,
+            "orbital_steps_per_s": n * n_states * steps / sec,
+            "sigma_dc_xx_at_E0": float(dc[0, i0]), "sigma_dc_yy_at_E0": float(dc[1, i0]),
+            "corr_dos_1": [float(corr_dos[0].real), float(corr_dos[0].imag)]}
+
+
+RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c5": run_c5}
 
 
 def main(argv=None) -> None:
@@ -185,7 +233,7 @@ def main(argv=None) -> None:
     for w in args.workloads:
         kw = {}
         if args.steps:
-            kw = {"steps": args.steps} if w in ("c1", "c3") else \
+            kw = {"steps": args.steps} if w in ("c1", "c3", "c5") else \
                  {"steps_dos": args.steps, "steps_ac": args.steps}
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
