@@ -225,6 +225,44 @@ int tbpm_cheb_timestep_noalloc(tbpm_ctx* ctx, const double* bes, int n_bes,
                                const double* hop, int64_t n_rows, int64_t nnz, double* wf,
                                int n_states, int forward);
 
+/* ---- learned C(t) tail extrapolator: BF16 kernels, FP32 accumulation ------
+ * No counterpart in the reference (TBPLaS has no learned component).  All
+ * pointers are device pointers owned by the caller; `stream` is a
+ * cudaStream_t (NULL = default stream); calls are asynchronous.  BF16 arrays
+ * are __nv_bfloat16 (passed as void*).  Layouts are row-major; convolution
+ * activations are channel-last [batch][length][channels]. */
+
+/* C[M,N] = alpha * A[M,K] . B[N,K]^T + beta * C (A, B BF16 with K contiguous,
+ * 16-byte aligned rows: K, lda, ldb multiples of 8; C FP32).  Tensor cores
+ * (mma.sync m16n8k16 BF16 -> FP32). */
+int tbpm_nn_gemm_tn(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M,
+                    int N, int K, float alpha, float beta, void* stream);
+/* out[c][r] = in[r][c] (BF16) */
+int tbpm_nn_transpose_bf16(const void* in, int rows, int cols, void* out, void* stream);
+/* Xcol[(b*Lout + lo)][j*C + c] = X[b][lo*stride + j - pad][c], zero outside */
+int tbpm_nn_im2col(const void* X, int batch, int L, int C, int k, int stride, int pad,
+                   int Lout, void* Xcol, void* stream);
+/* dX[b][l][c] = sum of dXcol entries that im2col copied from X[b][l][c] (FP32) */
+int tbpm_nn_col2im(const float* dXcol, int batch, int L, int C, int k, int stride, int pad,
+                   int Lout, float* dX, void* stream);
+/* a = act(Z + bias) (act 0: identity, 1: GELU, erf form); pre (optional)
+ * receives Z + bias; outputs in BF16 and/or FP32 (either may be NULL). */
+int tbpm_nn_bias_act(const float* Z, const float* bias, int M, int N, int act, float* pre,
+                     void* out_bf16, float* out_f32, void* stream);
+/* dZ = dA * act'(pre), FP32 and/or BF16 output */
+int tbpm_nn_act_backward(const float* dA, const float* pre, int64_t n, int act, float* dZ,
+                         void* dZ_bf16, void* stream);
+/* out[n] = sum_m Z[m][n] (bias gradients) */
+int tbpm_nn_colsum(const float* Z, int M, int N, float* out, void* stream);
+/* loss = mean((pred - target)^2) (device double), grad = d loss / d pred
+ * (optional); work: device scratch of >= 256 doubles */
+int tbpm_nn_mse(const float* pred, const float* target, int64_t n, float* grad, double* work,
+                double* loss, void* stream);
+/* AdamW step on FP32 master weights (step counts from 1); optional BF16 copy */
+int tbpm_nn_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1,
+                 float b2, float eps, float weight_decay, int step, void* w_bf16, void* stream);
+int tbpm_nn_cast_bf16(const float* in, int64_t n, void* out, void* stream);
+
 /* ---- device-resident propagation session (benchmarks, batching) --------- */
 
 /* Start a DOS propagation of n_states random states (seed rule as

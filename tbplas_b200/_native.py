@@ -38,7 +38,9 @@ EXPORTED_SYMBOLS = (
     "tbpm_psi_t", "tbpm_random_states", "tbpm_fermi_cheb_coef",
     "tbpm_cheb_timestep", "tbpm_fermi_apply", "tbpm_session_dos_begin",
     "tbpm_session_advance", "tbpm_session_read", "tbpm_cheb_timestep_noalloc",
-    "tbpm_dos_segmented",
+    "tbpm_dos_segmented", "tbpm_nn_gemm_tn", "tbpm_nn_transpose_bf16", "tbpm_nn_im2col",
+    "tbpm_nn_col2im", "tbpm_nn_bias_act", "tbpm_nn_act_backward", "tbpm_nn_colsum",
+    "tbpm_nn_mse", "tbpm_nn_adam", "tbpm_nn_cast_bf16",
 )
 
 
@@ -117,6 +119,20 @@ _SIGNATURES = {
                                             _vp, _c_int, _c_int]),
     "tbpm_dos_segmented": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64, _vp,
                                     _c_int, _c_int, _c_int, _c_int, _c_int, _c_dbl, _vp, _vp]),
+    "tbpm_nn_gemm_tn": (_c_int, [_vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
+                                 ctypes.c_float, ctypes.c_float, _vp]),
+    "tbpm_nn_transpose_bf16": (_c_int, [_vp, _c_int, _c_int, _vp, _vp]),
+    "tbpm_nn_im2col": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                _vp, _vp]),
+    "tbpm_nn_col2im": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                _vp, _vp]),
+    "tbpm_nn_bias_act": (_c_int, [_vp, _vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp]),
+    "tbpm_nn_act_backward": (_c_int, [_vp, _vp, _c_i64, _c_int, _vp, _vp, _vp]),
+    "tbpm_nn_colsum": (_c_int, [_vp, _c_int, _c_int, _vp, _vp]),
+    "tbpm_nn_mse": (_c_int, [_vp, _vp, _c_i64, _vp, _vp, _vp, _vp]),
+    "tbpm_nn_adam": (_c_int, [_vp, _vp, _vp, _vp, _c_i64, ctypes.c_float, ctypes.c_float,
+                              ctypes.c_float, ctypes.c_float, ctypes.c_float, _c_int, _vp, _vp]),
+    "tbpm_nn_cast_bf16": (_c_int, [_vp, _c_i64, _vp, _vp]),
 }
 
 _lib = None
