@@ -220,20 +220,35 @@ class TailNet:
         self.in_scale = 1.0 / max(float(np.sqrt(np.mean(x ** 2))), 1e-12)
         self.out_scale = 1.0 / max(float(np.sqrt(np.mean(y ** 2))), 1e-12)
 
+    def _snapshot(self):
+        return [p["w"].clone() for p in self.params]
+
+    def _restore(self, snap) -> None:
+        for p, w in zip(self.params, snap):
+            p["w"].copy_(w)
+            self._cast(p)
+
     def train(self, x: np.ndarray, y: np.ndarray, epochs: int = 100, batch: int = 64,
               lr: float = 1e-3, weight_decay: float = 1e-4, seed: int = 0,
               x_val: Optional[np.ndarray] = None, y_val: Optional[np.ndarray] = None,
-              log=None) -> Dict[str, list]:
-        """x: (n, n_in, 2), y: (n, n_out, 2).  Cosine-decayed AdamW."""
+              patience: Optional[int] = None, log=None) -> Dict[str, list]:
+        """x: (n, n_in, 2), y: (n, n_out, 2).  Cosine-decayed AdamW.  With a
+        validation set the weights of the best validation epoch are kept
+        (early stopping after `patience` epochs without improvement)."""
         t = self.torch
         n = x.shape[0]
         batch = max(8, (min(batch, n) // 8) * 8)
         ys = (y.reshape(n, -1) * self.out_scale).astype(np.float32)
         rng = np.random.default_rng(seed)
-        hist = {"train": [], "val": []}
+        hist = {"train": [], "val": [], "best_epoch": -1}
         steps_per_epoch = max(1, n // batch)
         total = epochs * steps_per_epoch
         it = 0
+        best, best_snap, since = math.inf, None, 0
+        if x_val is not None:
+            best = self.mse(x_val, y_val)
+            best_snap = self._snapshot()
+            hist["val_initial"] = best
         for ep in range(epochs):
             perm = rng.permutation(n)
             acc = 0.0
@@ -249,10 +264,21 @@ class TailNet:
                 it += 1
             hist["train"].append(acc / steps_per_epoch)
             if x_val is not None:
-                hist["val"].append(self.mse(x_val, y_val))
+                v = self.mse(x_val, y_val)
+                hist["val"].append(v)
+                if v < best:
+                    best, best_snap, since = v, self._snapshot(), 0
+                    hist["best_epoch"] = ep
+                else:
+                    since += 1
             if log and (ep % max(1, epochs // 10) == 0 or ep == epochs - 1):
                 log(f"epoch {ep}: train {hist['train'][-1]:.4e}"
                     + (f" val {hist['val'][-1]:.4e}" if hist["val"] else ""))
+            if patience is not None and x_val is not None and since > patience:
+                break
+        if best_snap is not None:
+            self._restore(best_snap)
+            hist["val_best"] = best
         return hist
 
     def predict(self, x: np.ndarray) -> np.ndarray:

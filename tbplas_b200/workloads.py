@@ -220,7 +220,149 @@ def run_c5(steps: int = 2048, n_states: int = 8, nx: int = 4096, precision: str 
             "corr_dos_1": [float(corr_dos[0].real), float(corr_dos[0].imag)]}
 
 
-RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c5": run_c5}
+def _realisation(args):
+    nx, ny, w, vac, seed = args
+    s = make_graphene_sample(nx, ny, disorder=w, vacancy_rate=vac, rescale=10.0, seed=seed)
+    h = s.build_ham_csr()
+    return h.indptr.astype(np.int64), h.indices.astype(np.int32), h.data
+
+
+def _pack(parts):
+    offsets, ips, ixs, vals, nnz = [0], [], [], [], 0
+    for ip, ix, v in parts:
+        ips.append(ip[:-1] + nnz)
+        ixs.append(ix + offsets[-1])
+        vals.append(v)
+        nnz += v.size
+        offsets.append(offsets[-1] + ip.size - 1)
+    indptr = np.concatenate(ips + [np.array([nnz])]).astype(np.int32)
+    return indptr, np.concatenate(ixs).astype(np.int32), np.concatenate(vals), \
+        np.array(offsets, dtype=np.int64)
+
+
+def generate_curves(specs, n_states: int, tnr: int, precision: str, seed: int,
+                    pack: int = 16, workers=None):
+    """Per-state DOS correlations of graphene realisations specs = [(nx, ny,
+    W, vacancy_rate, seed)], propagated on the GPU in packs of `pack`
+    realisations.  Returns (n_real, n_states, tnr+1) complex128 and the GPU
+    seconds spent."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    workers = workers or min(8, os.cpu_count() or 1)
+    out, gpu_sec = [], 0.0
+    bes = bessel_series(math.pi)  # dt*rescale = pi for rescale 10 and dt = 2 pi / 20
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        for p0 in range(0, len(specs), pack):
+            parts = list(ex.map(_realisation, specs[p0:p0 + pack]))
+            ip, ix, hv, off = _pack(parts)
+            f2py.set_backend(precision=precision)
+            (corr, per), sec = _timed(lambda: f2py.tbpm_dos_segmented(
+                bes, ip, ix, hv, off, n_states, seed + p0, tnr, per_state=True))
+            gpu_sec += sec
+            out.append(per)
+    f2py.set_backend(precision="fp64")
+    return np.concatenate(out), gpu_sec
+
+
+def run_c4(n_train: int = 128, n_test: int = 8, nx: int = 512, n_states: int = 8,
+           n_ref_states: int = 64, tnr: int = 2048, n_in: int = 256, epochs: int = 200,
+           seed: int = 2024, data: str = None) -> dict:
+    """Learned tail extrapolator: train on GPU-generated C(t) of disordered
+    graphene with vacancies, then compare the DOS of (n_in propagated steps +
+    predicted tail) with plain propagation of n steps, against a converged
+    reference (n_ref_states states, 2048 steps) on held-out realisations.
+
+    Time-to-DOS: plain FP64 needs n steps with n_states states; the learned
+    path needs n_in FP32 steps of the same states plus one network inference.
+    `data`: npz cache of the generated curves (written when absent).
+    """
+    from .learned import TailNet, curves_to_xy, dos_l1, extend
+    res = {"workload": f"c4 learned tail: {nx}x{nx} graphene, W~U[0,3] eV, vacancies 0-2%, "
+                       f"{n_states} states, n_in={n_in} -> {tnr}",
+           "n_train_curves": n_train * n_states, "n_test_realisations": n_test}
+    if data and os.path.exists(data):
+        d = np.load(data)
+        train, ref, ev64, ev32 = d["train"], d["ref"], d["ev64"], d["ev32"]
+        t_gen, t64, t32 = float(d["t_gen"]), float(d["t64"]), float(d["t32"])
+    else:
+        rng = np.random.default_rng(seed)
+        mk = lambda k, s0: [(nx, nx, float(rng.uniform(0, 3)), float(rng.uniform(0, 0.02)),
+                             s0 + i) for i in range(k)]
+        train_specs = mk(n_train, 10_000)
+        test_specs = mk(n_test, 20_000)
+        train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1)
+        ref32, _ = generate_curves(test_specs, n_ref_states, tnr, "fp32", 7)
+        ref = ref32.mean(axis=1)
+        ev64, t64 = generate_curves(test_specs, n_states, tnr, "fp64", 7)  # same first states
+        ev32, t32 = generate_curves(test_specs, n_states, tnr, "fp32", 7)
+        if data:
+            np.savez(data, train=train.astype(np.complex64), ref=ref, ev64=ev64, ev32=ev32,
+                     t_gen=t_gen, t64=t64, t32=t32)
+    res["datagen_gpu_seconds"] = t_gen
+    e_range = 20.0
+    c64 = ev64.mean(axis=1)
+    c32 = ev32.mean(axis=1)
+    l1 = lambda cs: float(np.mean([dos_l1(cs[k], ref[k], e_range) for k in range(n_test)]))
+    plain = {n: l1(c64[:, :n + 1]) for n in (128, 192, 256, 320, 384, 512, 768, 1024, 1536, 2048)}
+    res["l1_plain_fp64"] = {str(k): v for k, v in plain.items()}
+    res["l1_zero_tail_full_window"] = l1(np.concatenate(
+        [c32[:, :n_in + 1], np.zeros((n_test, tnr - n_in), complex)], axis=1))
+    sec_step64 = t64 / (n_test * tnr)
+    sec_step32 = t32 / (n_test * tnr)
+    res["seconds_per_step_fp64"] = sec_step64
+    res["seconds_per_step_fp32"] = sec_step32
+    variants = {
+        "per_state_wd1e-2": dict(targets="state", wd=1e-2),
+        "state_mean_wd1e-2": dict(targets="mean", wd=1e-2),
+        "per_state_wd1e-1": dict(targets="state", wd=1e-1),
+    }
+    best_name, best_l1 = None, math.inf
+    for name, v in variants.items():
+        if v["targets"] == "state":
+            x, y = curves_to_xy(train.reshape(-1, tnr + 1).astype(np.complex128), n_in,
+                                tnr - n_in)
+        else:
+            x, y = curves_to_xy(train.mean(axis=1).astype(np.complex128), n_in, tnr - n_in)
+        n_val = max(8, len(x) // 8)
+        net = TailNet(n_in=n_in, n_out=tnr - n_in, seed=seed)
+        net.fit_scales(x, y)
+        hist, t_train = _timed(lambda: net.train(x[n_val:], y[n_val:], epochs=epochs, batch=64,
+                                                 lr=1e-3, weight_decay=v["wd"],
+                                                 x_val=x[:n_val], y_val=y[:n_val],
+                                                 patience=30))
+        if v["targets"] == "state":
+            xs, _ = curves_to_xy(ev32.reshape(-1, tnr + 1), n_in, tnr - n_in)
+            tail, t_inf = _timed(lambda: net.predict(xs))
+            tail = tail.reshape(n_test, n_states, tnr - n_in, 2).mean(axis=1)
+        else:
+            xs, _ = curves_to_xy(c32, n_in, tnr - n_in)
+            tail, t_inf = _timed(lambda: net.predict(xs))
+        learned = extend(c32[:, :n_in + 1], tail)
+        r = {"train_seconds": t_train, "best_epoch": hist["best_epoch"],
+             "val_mse_initial": hist.get("val_initial"), "val_mse_best": hist.get("val_best"),
+             "l1_learned": l1(learned), "inference_seconds": t_inf}
+        res[f"variant_{name}"] = r
+        if r["l1_learned"] < best_l1:
+            best_name, best_l1 = name, r["l1_learned"]
+            t_learned = n_in * sec_step32 + t_inf / n_test
+    res["best_variant"] = best_name
+    res["l1_learned"] = best_l1
+    res["seconds_learned_per_realisation"] = t_learned
+    n_best_plain = min(plain, key=plain.get)
+    res["plain_best_steps"] = n_best_plain
+    res["plain_best_l1"] = plain[n_best_plain]
+    reach = [n for n in sorted(plain) if plain[n] <= best_l1]
+    if reach:
+        res["plain_steps_to_reach_learned_l1"] = reach[0]
+        res["time_to_dos_speedup_learned_vs_plain_fp64"] = reach[0] * sec_step64 / t_learned
+    else:
+        res["plain_steps_to_reach_learned_l1"] = None
+        res["time_to_dos_speedup_learned_vs_plain_fp64"] = None
+    res["speedup_vs_full_plain_2048_fp64"] = tnr * sec_step64 / t_learned
+    return res
+
+
+RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c5": run_c5}
 
 
 def main(argv=None) -> None:
@@ -229,12 +371,15 @@ def main(argv=None) -> None:
     ap.add_argument("--steps", type=int, default=None,
                     help="override the number of time steps (shorter runs)")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--data", default=None, help="c4: npz cache of the generated curves")
     args = ap.parse_args(argv)
     for w in args.workloads:
         kw = {}
         if args.steps:
             kw = {"steps": args.steps} if w in ("c1", "c3", "c5") else \
                  {"steps_dos": args.steps, "steps_ac": args.steps}
+        if w == "c4" and args.data:
+            kw["data"] = args.data
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
         print(line, flush=True)

@@ -113,3 +113,41 @@ def test_training_reduces_loss():
     net.train(x, y, epochs=60, batch=32, lr=2e-3)
     after = net.mse(x, y)
     assert after < 0.05 * before
+
+
+def test_learned_tail_beats_truncation_when_the_tail_is_deterministic():
+    """Weakly disordered graphene averaged over many states: C(t) beyond the
+    short window still carries the DOS fine structure.  A network trained on
+    GPU-generated curves of other realisations must give a DOS closer to the
+    full-length propagation than the DOS of the short window alone."""
+    import math
+    import tbplas_b200 as tb
+    from tbplas_b200.fortran import f2py
+    from tbplas_b200.learned import TailNet, curves_to_xy, dos_l1, extend
+    from conftest import bessel_series
+    n_in, tnr, ns = 64, 512, 64
+    rng = np.random.default_rng(5)
+
+    def batch(n, seed0):
+        samples = [tb.make_graphene_sample(48, 48, disorder=float(rng.uniform(0, 0.2)),
+                                           rescale=10.0, seed=seed0 + i) for i in range(n)]
+        p = tb.pack_samples(samples)
+        f2py.set_backend(precision="fp32")
+        try:
+            return f2py.tbpm_dos_segmented(bessel_series(math.pi), p.indptr, p.indices, p.data,
+                                           p.offsets, ns, seed0, tnr)
+        finally:
+            f2py.set_backend(precision="fp64")
+
+    train = batch(96, 100)
+    test = batch(16, 900)
+    x, y = curves_to_xy(train, n_in, tnr - n_in)
+    net = TailNet(n_in=n_in, n_out=tnr - n_in, width=64, seed=3)
+    net.fit_scales(x, y)
+    net.train(x[16:], y[16:], epochs=300, batch=16, lr=1e-3, weight_decay=1e-3,
+              x_val=x[:16], y_val=y[:16], patience=60)
+    xs, _ = curves_to_xy(test, n_in, tnr - n_in)
+    learned = extend(test[:, :n_in + 1], net.predict(xs))
+    l1_learned = np.mean([dos_l1(learned[k], test[k], 20.0) for k in range(16)])
+    l1_trunc = np.mean([dos_l1(test[k, :n_in + 1], test[k], 20.0) for k in range(16)])
+    assert l1_learned < 0.8 * l1_trunc, (l1_learned, l1_trunc)
