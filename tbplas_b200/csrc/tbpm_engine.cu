@@ -687,12 +687,13 @@ void dos_batch(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys* keys,
 // One DOS propagation of n_seg packed realisations x ns states each.  corr:
 // complex [n_seg][n_timestep+1], averaged over the ns states of a realisation;
 // corr_per_state (optional): complex [n_seg][ns][n_timestep+1].  The whole
-// propagation is captured as a single CUDA graph and launched once.
-template <typename R>
+// propagation is captured as a single CUDA graph and launched once.  V only
+// changes how term-kernel threads map onto the columns of a row; the
+// row-interleaved layout read by the segment kernels is the same for every V.
+template <typename R, int V>
 void dos_segmented_run(tbpm_ctx* c, const Expansion& ex, const std::vector<int64_t>& off,
                        int ns, int seed, int n_timestep, int chk_step, double chk_thr,
                        double* corr, double* corr_per_state) {
-  constexpr int V = 1;
   using C = typename Cx<R>::t;
   const int n_seg = (int)off.size() - 1;
   const int64_t n = c->ham.n;
@@ -1424,12 +1425,12 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
   c->launches = 0;
   c->model_bytes = 0;
   const Expansion ex = time_step_expansion(bes, n_bes);
-  if (c->ham.prec == TBPM_PREC_FP64)
-    dos_segmented_run<double>(c, ex, off, n_states, seed, n_timestep, chk_step, chk_thr, corr,
-                              corr_per_state);
-  else
-    dos_segmented_run<float>(c, ex, off, n_states, seed, n_timestep, chk_step, chk_thr, corr,
-                             corr_per_state);
+  dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states, c->opts.vector_width),
+           [&](auto tag) {
+             using P = decltype(tag);
+             dos_segmented_run<typename P::Real, P::V>(c, ex, off, n_states, seed, n_timestep,
+                                                       chk_step, chk_thr, corr, corr_per_state);
+           });
 }
 
 void drv_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const double* psi0,

@@ -264,32 +264,72 @@ def generate_curves(specs, n_states: int, tnr: int, precision: str, seed: int,
     return np.concatenate(out), gpu_sec
 
 
+def _l1_mean(curves, refs, e_range: float = 20.0) -> float:
+    from .learned import dos_l1 as l1
+    return float(np.mean([l1(curves[k], refs[k], e_range) for k in range(len(refs))]))
+
+
+def _time_dos_paths(parts, n_states: int, steps_list, seed: int = 7) -> dict:
+    """End-to-end seconds per realisation (host CSR in, correlation out) of
+    the plain FP64 path (f2py.tbpm_dos, one realisation per call) and of the
+    FP32 path with all realisations packed into one launch, for each number
+    of steps in steps_list."""
+    bes = bessel_series(math.pi)
+    ip1, ix1, hv1 = parts[0]
+    ip, ix, hv, off = _pack(parts)
+    out = {}
+    try:
+        for n in steps_list:
+            f2py.set_backend(precision="fp64")
+            f2py.tbpm_dos(bes, ip1, ix1, hv1, seed, 8, n_states, "", 0, 1024, 1e-9)  # warm-up
+            _, t64 = _timed(lambda: f2py.tbpm_dos(bes, ip1, ix1, hv1, seed, n, n_states, "", 0,
+                                                  1 << 30, 1e-9))
+            f2py.set_backend(precision="fp32")
+            f2py.tbpm_dos_segmented(bes, ip, ix, hv, off, n_states, seed, 8)  # warm-up
+            _, t32 = _timed(lambda: f2py.tbpm_dos_segmented(bes, ip, ix, hv, off, n_states,
+                                                            seed, n, 1 << 30))
+            out[n] = {"plain_fp64_seconds": t64, "fp32_batched_seconds": t32 / len(parts)}
+    finally:
+        f2py.set_backend(precision="fp64")
+    return out
+
+
+def _steps_to_reach(l1_by_steps: dict, target: float):
+    ok = [n for n in sorted(l1_by_steps) if l1_by_steps[n] < target]
+    return ok[0] if ok else None
+
+
 def run_c4(n_train: int = 128, n_test: int = 8, nx: int = 512, n_states: int = 8,
            n_ref_states: int = 64, tnr: int = 2048, n_in: int = 256, epochs: int = 200,
-           seed: int = 2024, data: str = None) -> dict:
-    """Learned tail extrapolator: train on GPU-generated C(t) of disordered
-    graphene with vacancies, then compare the DOS of (n_in propagated steps +
-    predicted tail) with plain propagation of n steps, against a converged
-    reference (n_ref_states states, 2048 steps) on held-out realisations.
+           seed: int = 2024, data: str = None, target_l1: float = 1e-3) -> dict:
+    """Learned tail extrapolator on disordered graphene with vacancies.
 
-    Time-to-DOS: plain FP64 needs n steps with n_states states; the learned
-    path needs n_in FP32 steps of the same states plus one network inference.
-    `data`: npz cache of the generated curves (written when absent).
+    Trains on GPU-generated C(t) (FP32, n_states states per realisation),
+    then compares on held-out realisations the DOS of
+      * plain FP64 propagation of n steps,
+      * FP32 propagation of n steps, realisations packed into one launch,
+      * n_in FP32 steps followed by the predicted tail (learned),
+    with two error definitions: L1 against the full tnr-step FP64
+    propagation of the same states, and L1 against a converged reference
+    (n_ref_states states).  Time-to-DOS at L1 < target_l1 (same-state
+    definition) uses end-to-end timings of each path.  `data`: npz cache of
+    the generated curves (written when absent).
     """
-    from .learned import TailNet, curves_to_xy, dos_l1, extend
+    from .learned import TailNet, curves_to_xy, extend
     res = {"workload": f"c4 learned tail: {nx}x{nx} graphene, W~U[0,3] eV, vacancies 0-2%, "
                        f"{n_states} states, n_in={n_in} -> {tnr}",
-           "n_train_curves": n_train * n_states, "n_test_realisations": n_test}
+           "n_train_curves": n_train * n_states, "n_test_realisations": n_test,
+           "target_l1": target_l1}
+    rng = np.random.default_rng(seed)
+    mk = lambda k, s0: [(nx, nx, float(rng.uniform(0, 3)), float(rng.uniform(0, 0.02)),
+                         s0 + i) for i in range(k)]
+    train_specs = mk(n_train, 10_000)
+    test_specs = mk(n_test, 20_000)
     if data and os.path.exists(data):
         d = np.load(data)
         train, ref, ev64, ev32 = d["train"], d["ref"], d["ev64"], d["ev32"]
-        t_gen, t64, t32 = float(d["t_gen"]), float(d["t64"]), float(d["t32"])
+        t_gen = float(d["t_gen"])
     else:
-        rng = np.random.default_rng(seed)
-        mk = lambda k, s0: [(nx, nx, float(rng.uniform(0, 3)), float(rng.uniform(0, 0.02)),
-                             s0 + i) for i in range(k)]
-        train_specs = mk(n_train, 10_000)
-        test_specs = mk(n_test, 20_000)
         train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1)
         ref32, _ = generate_curves(test_specs, n_ref_states, tnr, "fp32", 7)
         ref = ref32.mean(axis=1)
@@ -299,24 +339,23 @@ def run_c4(n_train: int = 128, n_test: int = 8, nx: int = 512, n_states: int = 8
             np.savez(data, train=train.astype(np.complex64), ref=ref, ev64=ev64, ev32=ev32,
                      t_gen=t_gen, t64=t64, t32=t32)
     res["datagen_gpu_seconds"] = t_gen
-    e_range = 20.0
     c64 = ev64.mean(axis=1)
     c32 = ev32.mean(axis=1)
-    l1 = lambda cs: float(np.mean([dos_l1(cs[k], ref[k], e_range) for k in range(n_test)]))
-    plain = {n: l1(c64[:, :n + 1]) for n in (128, 192, 256, 320, 384, 512, 768, 1024, 1536, 2048)}
-    res["l1_plain_fp64"] = {str(k): v for k, v in plain.items()}
-    res["l1_zero_tail_full_window"] = l1(np.concatenate(
-        [c32[:, :n_in + 1], np.zeros((n_test, tnr - n_in), complex)], axis=1))
-    sec_step64 = t64 / (n_test * tnr)
-    sec_step32 = t32 / (n_test * tnr)
-    res["seconds_per_step_fp64"] = sec_step64
-    res["seconds_per_step_fp32"] = sec_step32
+    grid = (128, 256, 384, 512, 768, 1024, 1536, 1792, 1920, tnr)
+    same64 = {n: _l1_mean(c64[:, :n + 1], c64) for n in grid}
+    same32 = {n: _l1_mean(c32[:, :n + 1], c64) for n in grid}
+    conv64 = {n: _l1_mean(c64[:, :n + 1], ref) for n in grid}
+    res["l1_same_states_plain_fp64"] = {str(k): v for k, v in same64.items()}
+    res["l1_same_states_fp32"] = {str(k): v for k, v in same32.items()}
+    res["l1_converged_plain_fp64"] = {str(k): v for k, v in conv64.items()}
+    res["l1_converged_reference_vs_same_states_full"] = _l1_mean(ref, c64)
+
     variants = {
         "per_state_wd1e-2": dict(targets="state", wd=1e-2),
         "state_mean_wd1e-2": dict(targets="mean", wd=1e-2),
         "per_state_wd1e-1": dict(targets="state", wd=1e-1),
     }
-    best_name, best_l1 = None, math.inf
+    best = None
     for name, v in variants.items():
         if v["targets"] == "state":
             x, y = curves_to_xy(train.reshape(-1, tnr + 1).astype(np.complex128), n_in,
@@ -340,29 +379,133 @@ def run_c4(n_train: int = 128, n_test: int = 8, nx: int = 512, n_states: int = 8
         learned = extend(c32[:, :n_in + 1], tail)
         r = {"train_seconds": t_train, "best_epoch": hist["best_epoch"],
              "val_mse_initial": hist.get("val_initial"), "val_mse_best": hist.get("val_best"),
-             "l1_learned": l1(learned), "inference_seconds": t_inf}
+             "l1_same_states": _l1_mean(learned, c64), "l1_converged": _l1_mean(learned, ref),
+             "inference_seconds_per_realisation": t_inf / n_test}
         res[f"variant_{name}"] = r
-        if r["l1_learned"] < best_l1:
-            best_name, best_l1 = name, r["l1_learned"]
-            t_learned = n_in * sec_step32 + t_inf / n_test
-    res["best_variant"] = best_name
-    res["l1_learned"] = best_l1
-    res["seconds_learned_per_realisation"] = t_learned
-    n_best_plain = min(plain, key=plain.get)
-    res["plain_best_steps"] = n_best_plain
-    res["plain_best_l1"] = plain[n_best_plain]
-    reach = [n for n in sorted(plain) if plain[n] <= best_l1]
-    if reach:
-        res["plain_steps_to_reach_learned_l1"] = reach[0]
-        res["time_to_dos_speedup_learned_vs_plain_fp64"] = reach[0] * sec_step64 / t_learned
-    else:
-        res["plain_steps_to_reach_learned_l1"] = None
-        res["time_to_dos_speedup_learned_vs_plain_fp64"] = None
-    res["speedup_vs_full_plain_2048_fp64"] = tnr * sec_step64 / t_learned
+        if best is None or r["l1_same_states"] < best[1]["l1_same_states"]:
+            best = (name, r)
+    res["best_variant"] = best[0]
+    res["l1_same_states_learned"] = best[1]["l1_same_states"]
+    res["l1_converged_learned"] = best[1]["l1_converged"]
+    res["l1_same_states_truncated_at_n_in_fp32"] = same32[n_in]
+    zero = np.zeros((n_test, tnr - n_in, 2))
+    res["l1_same_states_zero_tail_fp32"] = _l1_mean(extend(c32[:, :n_in + 1], zero), c64)
+
+    # time-to-DOS, same-state definition
+    parts = [_realisation(sp) for sp in test_specs]
+    n64 = _steps_to_reach(same64, target_l1)
+    n32 = _steps_to_reach(same32, target_l1)
+    need = sorted({n for n in (n64, n32, n_in) if n})
+    times = _time_dos_paths(parts, n_states, need)
+    res["seconds_per_realisation"] = {str(k): v for k, v in times.items()}
+    t_plain = times[n64]["plain_fp64_seconds"] if n64 else None
+    t_fp32 = times[n32]["fp32_batched_seconds"] if n32 else None
+    learned_ok = best[1]["l1_same_states"] < target_l1
+    t_learned = (times[n_in]["fp32_batched_seconds"] + best[1]["inference_seconds_per_realisation"]
+                 if learned_ok else None)
+    res["time_to_dos"] = {
+        "plain_fp64": {"steps": n64, "seconds_per_realisation": t_plain},
+        "fp32_batched": {"steps": n32, "seconds_per_realisation": t_fp32},
+        "fp32_batched_learned": {"reached": learned_ok, "steps": n_in if learned_ok else None,
+                                 "seconds_per_realisation": t_learned},
+    }
+    res["time_to_dos_speedup_fp32_batched_vs_plain_fp64"] = (
+        t_plain / t_fp32 if t_plain and t_fp32 else None)
+    res["time_to_dos_speedup_learned_vs_plain_fp64"] = (
+        t_plain / t_learned if t_plain and t_learned else None)
+    # the best plain accuracy against the converged reference, and what the
+    # learned tail reaches there
+    n_best = min(conv64, key=conv64.get)
+    res["converged_best_plain_steps"] = n_best
+    res["converged_best_plain_l1"] = conv64[n_best]
     return res
 
 
-RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c5": run_c5}
+def run_c4c(n_train: int = 96, n_test: int = 16, nx: int = 48, n_states: int = 64,
+            nx_test: int = None, n_states_test: int = None, pack_test: int = None,
+            tnr: int = 512, n_in: int = 64, w_max: float = 0.2, width: int = 64,
+            epochs: int = 300, seed: int = 5, target_l1: float = 1e-3) -> dict:
+    """The learned tail where C(t) carries a deterministic tail: weakly
+    disordered graphene (W ~ U[0, w_max] eV, no vacancies) whose DOS keeps
+    sharp structure at full resolution.  The network is trained on the state
+    averages of nx x nx realisations (n_states states each); held-out
+    nx_test x nx_test realisations (n_states_test states) are propagated
+    n_in steps in FP32 and extended by the predicted tail.  All DOS L1 errors
+    are against the full tnr-step FP64 propagation of the same states.
+
+    Timings are end to end per realisation: the FP64 reference run (one
+    launch per pack_test realisations) gives the plain path, scaled to n
+    steps where fewer suffice; the FP32 n_in-step run plus inference gives
+    the learned path."""
+    from .learned import TailNet, curves_to_xy, extend
+    nx_test = nx_test or nx
+    n_states_test = n_states_test or n_states
+    pack_test = pack_test or n_test
+    rng = np.random.default_rng(seed)
+    mk = lambda k, s0, n: [(n, n, float(rng.uniform(0, w_max)), 0.0, s0 + i) for i in range(k)]
+    train_specs = mk(n_train, 100, nx)
+    test_specs = mk(n_test, 900, nx_test)
+    pack_train = max(1, min(n_train, (1 << 23) // (2 * nx * nx)))
+    train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1, pack=pack_train)
+    ev64, t64 = generate_curves(test_specs, n_states_test, tnr, "fp64", 7, pack=pack_test)
+    ev32, t32 = generate_curves(test_specs, n_states_test, n_in, "fp32", 7, pack=pack_test)
+    c64, c32 = ev64.mean(axis=1), ev32.mean(axis=1)
+    x, y = curves_to_xy(train.mean(axis=1), n_in, tnr - n_in)
+    n_val = max(8, n_train // 6)
+    net = TailNet(n_in=n_in, n_out=tnr - n_in, width=width, seed=3)
+    net.fit_scales(x, y)
+    hist, t_train = _timed(lambda: net.train(x[n_val:], y[n_val:], epochs=epochs, batch=16,
+                                             lr=1e-3, weight_decay=1e-3, x_val=x[:n_val],
+                                             y_val=y[:n_val], patience=60))
+    xs, _ = curves_to_xy(c32, n_in, tnr - n_in)
+    tail, t_inf = _timed(lambda: net.predict(xs))
+    learned = extend(c32, tail)
+    grid = sorted({n_in, 2 * n_in, 3 * n_in, 4 * n_in, tnr // 2, 3 * tnr // 4, 7 * tnr // 8, tnr})
+    plain = {n: _l1_mean(c64[:, :n + 1], c64) for n in grid}
+    l1_learned = _l1_mean(learned, c64)
+    n_match = _steps_to_reach(plain, l1_learned)
+    n_target = _steps_to_reach(plain, target_l1)
+    t_plain_full = t64 / n_test
+    t_learned = t32 / n_test + t_inf / n_test
+    per_step = lambda n: t_plain_full * n / tnr if n else None
+    return {"workload": f"c4c coherent tail: train {nx}x{nx} graphene x {n_states} states, "
+                        f"test {nx_test}x{nx_test} x {n_states_test} states, "
+                        f"W~U[0,{w_max}] eV, n_in={n_in} -> {tnr}",
+            "n_train_realisations": n_train, "n_test_realisations": n_test,
+            "datagen_gpu_seconds": t_gen, "train_seconds": t_train,
+            "best_epoch": hist["best_epoch"], "val_mse_initial": hist.get("val_initial"),
+            "val_mse_best": hist.get("val_best"),
+            "l1_same_states_plain_fp64": {str(k): v for k, v in plain.items()},
+            "l1_same_states_truncated_at_n_in_fp32": _l1_mean(c32, c64),
+            "l1_same_states_zero_tail_fp32": _l1_mean(
+                extend(c32, np.zeros((n_test, tnr - n_in, 2))), c64),
+            "l1_same_states_learned": l1_learned,
+            "plain_steps_to_match_learned": n_match,
+            "plain_fp64_seconds_per_realisation_full": t_plain_full,
+            "learned_seconds_per_realisation": t_learned,
+            "time_to_dos_speedup_learned_vs_plain_fp64_at_learned_l1": (
+                per_step(n_match) / t_learned if n_match else None),
+            "target_l1": target_l1,
+            "learned_reaches_target": l1_learned < target_l1,
+            "plain_steps_to_reach_target": n_target,
+            "time_to_dos_speedup_learned_vs_plain_fp64_at_target": (
+                per_step(n_target) / t_learned if (n_target and l1_learned < target_l1)
+                else None)}
+
+
+def run_c4l(**kw) -> dict:
+    """c4c at scale: the tail learned on 512^2 realisations (16 states,
+    ballistic range of 512 steps ~ 430 cells stays inside the sample), tested
+    on 2048^2 realisations with 64 states, where the stochastic part of the
+    tail is small enough for a DOS L1 near 1e-3."""
+    args = dict(n_train=256, n_test=2, nx=512, n_states=16, nx_test=2048, n_states_test=64,
+                pack_test=1, w_max=0.5, width=128, epochs=300)
+    args.update(kw)
+    return run_c4c(**args)
+
+
+RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c4c": run_c4c, "c4l": run_c4l,
+           "c5": run_c5}
 
 
 def main(argv=None) -> None:
