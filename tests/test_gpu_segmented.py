@@ -27,11 +27,12 @@ def _realisations():
             for i, (nx, ny, w, v) in enumerate(specs)]
 
 
+@pytest.mark.parametrize("ns", [3, 4])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 3e-5)])
-def test_segmented_matches_separate_oracle_runs(prec, tol):
+def test_segmented_matches_separate_oracle_runs(prec, tol, ns):
     samples = _realisations()
     packed = tb.pack_samples(samples)
-    ns, tnr, seed = 3, 40, 1337
+    tnr, seed = 40, 1337
     bes = bessel_series(2 * math.pi / packed.energy_range * packed.rescale)
     f2py.set_backend(precision=prec, device=0)
     try:
