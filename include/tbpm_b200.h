@@ -94,6 +94,65 @@ int tbpm_ham_upload(tbpm_ctx* ctx, const int32_t* indptr, const int32_t* indices
                     const double* dy, double rescale);
 int tbpm_ham_release(tbpm_ctx* ctx);
 
+/* ---- supercell Hamiltonian assembled on the device ------------------------ */
+
+/* entry layouts */
+#define TBPM_LAYOUT_CSR 0 /* Sample.build_ham_csr (builder/sample.py:375-391):
+                             columns sorted, on-site terms != 0, zeros dropped */
+#define TBPM_LAYOUT_DXY 1 /* Sample.build_ham_dxy, algo "fast"
+                             (cython/sample.pyx:150-257): on-site term first when
+                             |E| >= cutoff, then hopping terms in the reference's
+                             list order, with dx, dy */
+
+/* A periodic supercell of a primitive cell, in the arrays a tbplas
+ * PrimitiveCell / SuperCell / Sample hold (builder/primitive.py:957-1055,
+ * builder/super.py:848-912).  Host pointers. */
+typedef struct tbpm_supercell {
+  const double* lat_vec;    /* [3][3] lattice vectors of the primitive cell (rows), nm */
+  const double* origin;     /* [3] lattice origin, nm (NULL: 0) */
+  int n_orb;                /* orbitals in the primitive cell */
+  const double* orb_pos;    /* [n_orb][3] fractional orbital positions */
+  const double* orb_eng;    /* [n_orb] on-site energies, eV */
+  int n_hop;                /* reduced hopping terms (PrimitiveCell.hop_ind) */
+  const int32_t* hop_ind;   /* [n_hop][5]: ra, rb, rc, bra orbital, ket orbital */
+  const double* hop_eng;    /* [n_hop] complex (re, im) hopping energies, eV */
+  int32_t dim[3];           /* supercell dimension */
+  int32_t pbc[3];           /* periodic boundary conditions (0/1) */
+  const int64_t* vac_id_sc; /* sorted, unique vacancy indices, numbering
+                               ((ia*dim[1] + ib)*dim[2] + ic)*n_orb + o; NULL: none */
+  int64_t n_vac;
+  const double* sc_orb_eng; /* optional [n_rows] on-site energies of the supercell
+                               orbitals in eV before rescaling (Sample.orb_eng, e.g.
+                               with disorder); NULL: primitive-cell values */
+  double b_field;           /* Peierls field along -z in Tesla (0: none), applied
+                               before rescaling as Sample.set_magnetic_field */
+  int gauge;                /* 0, 1 or 2 (cython/sample.pyx:20-74) */
+  double rescale;           /* > 0: Sample.rescale_ham(rescale); <= 0: estimated
+                               like Sample.get_rescale (cython/sample.pyx:77-116) */
+} tbpm_supercell;
+
+/* Assemble the Hamiltonian of a supercell on the device and keep it resident
+ * in the context, in place of Sample.build_ham_csr / build_ham_dxy + a host
+ * CSR upload (tbpm_ham_upload).  The TBPM drivers then run on it with
+ * indptr == NULL.  layout: TBPM_LAYOUT_CSR for DOS / LDOS / psi_t,
+ * TBPM_LAYOUT_DXY (with dx, dy) for AC / DC; orb_eng_cutoff is the DXY
+ * on-site cutoff (eV after rescaling, reference default 1e-5).
+ * Returns the row count, the entry count of the full CSR and the rescale
+ * factor used.  Positions, dr, the rescale estimate and field-free values are
+ * bit-identical to the reference builder; Peierls factors are within 2 ulp. */
+int tbpm_supercell_ham(tbpm_ctx* ctx, const tbpm_supercell* sc, int layout,
+                       double orb_eng_cutoff, int64_t* n_rows, int64_t* nnz,
+                       double* rescale);
+
+/* As tbpm_supercell_ham, but copies the full CSR of the layout to host
+ * arrays: indptr int64[n_rows+1], indices int32[nnz], hop complex128[nnz],
+ * dx, dy float64[nnz] (DXY only; may be NULL).  With indptr == NULL only
+ * n_rows, nnz and rescale are returned (call twice to size the arrays). */
+int tbpm_supercell_csr(tbpm_ctx* ctx, const tbpm_supercell* sc, int layout,
+                       double orb_eng_cutoff, int64_t* n_rows, int64_t* nnz, double* rescale,
+                       int64_t* indptr, int32_t* indices, double* hop, double* dx,
+                       double* dy);
+
 /* ---- f2py-equivalent drivers (host buffers in, host buffers out) --------- */
 
 /* tbpm_dos -- replaces tbpm.f90:6-93 (SUBROUTINE tbpm_dos) as called from

@@ -7,9 +7,11 @@ propagation and correlation loops as CUDA kernels in libtbpm_b200.so.
 from .base import EPSILON0, H_BAR_EV, KB
 from .builder import LatticeSample, PackedSamples, make_graphene_sample, pack_samples
 from .parallel import MPIEnv
+from .supercell import DeviceSample, make_graphene_device_sample
 from .tbpm import (Analyzer, Config, Solver, read_config, window_exp, window_exp_ten,
                    window_hanning)
 
 __all__ = ["Config", "read_config", "Solver", "Analyzer", "window_hanning", "window_exp",
            "window_exp_ten", "LatticeSample", "make_graphene_sample", "pack_samples",
-           "PackedSamples", "MPIEnv", "KB", "H_BAR_EV", "EPSILON0"]
+           "PackedSamples", "MPIEnv", "KB", "H_BAR_EV", "EPSILON0", "DeviceSample",
+           "make_graphene_device_sample"]

@@ -28,6 +28,8 @@ PREC_FP64 = 0
 PREC_FP32 = 1
 STATE_EXP = 0
 STATE_UNIT = 1
+LAYOUT_CSR = 0
+LAYOUT_DXY = 1
 
 # every symbol include/tbpm_b200.h declares
 EXPORTED_SYMBOLS = (
@@ -40,7 +42,8 @@ EXPORTED_SYMBOLS = (
     "tbpm_session_advance", "tbpm_session_read", "tbpm_cheb_timestep_noalloc",
     "tbpm_dos_segmented", "tbpm_nn_gemm_tn", "tbpm_nn_transpose_bf16", "tbpm_nn_im2col",
     "tbpm_nn_col2im", "tbpm_nn_bias_act", "tbpm_nn_act_backward", "tbpm_nn_colsum",
-    "tbpm_nn_mse", "tbpm_nn_adam", "tbpm_nn_cast_bf16",
+    "tbpm_nn_mse", "tbpm_nn_adam", "tbpm_nn_cast_bf16", "tbpm_supercell_ham",
+    "tbpm_supercell_csr",
 )
 
 
@@ -75,6 +78,29 @@ _c_int = ctypes.c_int
 _c_i64 = ctypes.c_int64
 _c_dbl = ctypes.c_double
 _vp = ctypes.c_void_p
+
+
+class Supercell(ctypes.Structure):
+    """struct tbpm_supercell (host pointers into numpy arrays kept alive by the
+    caller)."""
+    _fields_ = [
+        ("lat_vec", _vp),
+        ("origin", _vp),
+        ("n_orb", _c_int),
+        ("orb_pos", _vp),
+        ("orb_eng", _vp),
+        ("n_hop", _c_int),
+        ("hop_ind", _vp),
+        ("hop_eng", _vp),
+        ("dim", ctypes.c_int32 * 3),
+        ("pbc", ctypes.c_int32 * 3),
+        ("vac_id_sc", _vp),
+        ("n_vac", _c_i64),
+        ("sc_orb_eng", _vp),
+        ("b_field", _c_dbl),
+        ("gauge", _c_int),
+        ("rescale", _c_dbl),
+    ]
 
 _SIGNATURES = {
     "tbpm_create": (_c_int, [_c_int, ctypes.POINTER(_vp)]),
@@ -133,6 +159,12 @@ _SIGNATURES = {
     "tbpm_nn_adam": (_c_int, [_vp, _vp, _vp, _vp, _c_i64, ctypes.c_float, ctypes.c_float,
                               ctypes.c_float, ctypes.c_float, ctypes.c_float, _c_int, _vp, _vp]),
     "tbpm_nn_cast_bf16": (_c_int, [_vp, _c_i64, _vp, _vp]),
+    "tbpm_supercell_ham": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,
+                                    ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64),
+                                    ctypes.POINTER(_c_dbl)]),
+    "tbpm_supercell_csr": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,
+                                    ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64),
+                                    ctypes.POINTER(_c_dbl), _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

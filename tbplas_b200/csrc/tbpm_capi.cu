@@ -39,6 +39,11 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
                        double chk_thr, double* corr, double* corr_per_state);
 void drv_session_advance(tbpm_ctx* c, int n_steps);
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done);
+void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
+                       int64_t* n_rows, int64_t* nnz, double* rescale);
+void drv_supercell_csr(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
+                       int64_t* n_rows, int64_t* nnz, double* rescale, int64_t* indptr,
+                       int32_t* indices, double* hop, double* dx, double* dy);
 }  // namespace tbpm
 
 namespace {
@@ -173,6 +178,24 @@ int tbpm_ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
                     const double* dy, double rescale) {
   return guarded(c, [&] {
     tbpm::drv_ham_upload(c, indptr, indices, hop, n_rows, nnz, dx, dy, rescale);
+  });
+}
+
+int tbpm_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout,
+                       double orb_eng_cutoff, int64_t* n_rows, int64_t* nnz,
+                       double* rescale) {
+  return guarded(c, [&] {
+    tbpm::drv_supercell_ham(c, sc, layout, orb_eng_cutoff, n_rows, nnz, rescale);
+  });
+}
+
+int tbpm_supercell_csr(tbpm_ctx* c, const tbpm_supercell* sc, int layout,
+                       double orb_eng_cutoff, int64_t* n_rows, int64_t* nnz, double* rescale,
+                       int64_t* indptr, int32_t* indices, double* hop, double* dx,
+                       double* dy) {
+  return guarded(c, [&] {
+    tbpm::drv_supercell_csr(c, sc, layout, orb_eng_cutoff, n_rows, nnz, rescale, indptr,
+                            indices, hop, dx, dy);
   });
 }
 

@@ -72,7 +72,14 @@ def _ctx() -> nat.Context:
 
 
 def _csr(indptr, indices, hop):
-    """f2py casts: INTEGER (int32) index arrays, COMPLEX(KIND=8) values."""
+    """f2py casts: INTEGER (int32) index arrays, COMPLEX(KIND=8) values.
+
+    In the place of indptr a handle of a device-assembled Hamiltonian
+    (tbplas_b200.supercell.ResidentHam) may be given: it is assembled in the
+    context and the drivers get NULL arrays (the resident Hamiltonian)."""
+    if hasattr(indptr, "make_resident"):
+        n, nnz = indptr.make_resident(_ctx())
+        return None, None, None, n, nnz
     indptr = np.asarray(indptr)
     indices = np.asarray(indices)
     if indptr.size and int(indptr.max()) > _INT32_MAX:
@@ -87,7 +94,9 @@ def _csr(indptr, indices, hop):
     return ip, ix, hv, ip.size - 1, hv.size
 
 
-def _real(a, n) -> np.ndarray:
+def _real(a, n) -> Optional[np.ndarray]:
+    if a is None:
+        return None
     r = nat.as_c(a, np.float64)
     if r.size != n:
         raise ValueError("dx/dy must have the same length as hop")

@@ -72,3 +72,28 @@ def test_f2py_argument_validation_happens_on_host():
         f2py.set_backend(precision="fp16")
     with pytest.raises(ValueError):
         f2py.set_backend(nonsense=1)
+
+
+def test_device_sample_interface_without_device_work():
+    """DeviceSample exposes the Sample interface the Solver and Analyzer read;
+    without a GPU its assembly raises instead of building on the host."""
+    s = tb.make_graphene_device_sample(4, 3, rescale=9.0)
+    ref = tb.LatticeSample((4, 3))
+    assert s.num_orb == ref.num_orb == 24
+    assert s.area_unit_cell == ref.area_unit_cell
+    assert s.volume_unit_cell == ref.volume_unit_cell
+    assert s.nr_orbitals == 2 and s.extended == 1.0
+    assert s.rescale == 9.0 and s.energy_range == 18.0
+    h = s.build_ham_csr()
+    assert hasattr(h.indptr, "make_resident") and h.shape == (24, 24)
+    ip, ix, hop, dx, dy = s.build_ham_dxy()
+    assert hasattr(ip, "make_resident") and ix is None and dx is None
+    with pytest.raises(ValueError):
+        tb.DeviceSample(np.eye(3), None, [[0, 0, 0]], [0.0, 1.0], [[1, 0, 0, 0, 0]], [-1.0],
+                        (3, 1, 1))
+    with pytest.raises(ValueError):
+        tb.make_graphene_device_sample(4, 3, gauge=5)
+    if not _gpu_present():
+        nat._contexts.clear()
+        with pytest.raises(nat.TbpmError):
+            s.download_ham_csr()
