@@ -28,7 +28,7 @@ import time
 import numpy as np
 
 from . import _native as nat
-from .builder import make_graphene_sample
+from .builder import LatticeSample, make_graphene_sample
 from .fortran import f2py
 from .tbpm import Analyzer, Config, Solver
 
@@ -173,48 +173,60 @@ def run_c3(steps: int = 512, n_states: int = 4, n_real: int = 64, lo: int = 256,
 
 
 def run_c5(steps: int = 2048, n_states: int = 8, nx: int = 4096, precision: str = "fp32",
-           energy_limits=(-0.5, 0.5)) -> dict:
+           energy_limits=(-0.5, 0.5), builder: str = "device") -> dict:
     """DC conductivity of 4096x4096 graphene in a perpendicular field of one
     flux quantum per 1024 hexagons (B = h/e / (1024 * hexagon area) = 77.06 T,
     Peierls phases in the gauge A = (By, 0, 0)), Anderson W = 1 eV, through the
-    drop-in Solver / Analyzer."""
+    drop-in Solver / Analyzer.  builder "device" assembles the Hamiltonian on
+    the GPU (DeviceSample), "host" builds the CSR with numpy and uploads it."""
     import tempfile
-    t0 = time.perf_counter()
-    s = make_graphene_sample(nx, nx, disorder=1.0, rescale=9.0, seed=1337)
+    from .supercell import make_graphene_device_sample
     flux_quantum = 4135.667  # h/e in T nm^2
-    b_field = flux_quantum / (1024 * s.area_unit_cell)
-    s.set_magnetic_field(b_field, gauge=0)
-    ham = s.build_ham_dxy()
-    t_build = time.perf_counter() - t0
+    b_field = flux_quantum / (1024 * LatticeSample((1, 1)).area_unit_cell)
+    t0 = time.perf_counter()
+    if builder == "device":
+        f2py.set_backend(precision=precision, batch=n_states)
+        sample = make_graphene_device_sample(nx, nx, disorder=1.0, b_field=b_field, gauge=0,
+                                             rescale=9.0, seed=1337)
+        n, _ = sample.build_ham_dxy()[0].make_resident(f2py._ctx())
+        t_build = time.perf_counter() - t0
+    else:
+        s = make_graphene_sample(nx, nx, disorder=1.0, rescale=9.0, seed=1337)
+        s.set_magnetic_field(b_field, gauge=0)
+        ham = s.build_ham_dxy()
+        t_build = time.perf_counter() - t0
+        n = ham[0].size - 1
 
-    class Prebuilt:  # the Sample interface with the arrays built once
-        rescale = s.rescale
-        energy_range = s.energy_range
-        nr_orbitals = s.nr_orbitals
-        area_unit_cell = s.area_unit_cell
-        volume_unit_cell = s.volume_unit_cell
-        extended = s.extended
+        class Prebuilt:  # the Sample interface with the arrays built once
+            rescale = s.rescale
+            energy_range = s.energy_range
+            nr_orbitals = s.nr_orbitals
+            area_unit_cell = s.area_unit_cell
+            volume_unit_cell = s.volume_unit_cell
+            extended = s.extended
 
-        def build_ham_dxy(self):
-            return ham
+            def build_ham_dxy(self):
+                return ham
+
+        sample = Prebuilt()
 
     cfg = Config()
     cfg.generic["nr_time_steps"] = steps
     cfg.generic["nr_random_samples"] = n_states
     cfg.DC_conductivity["energy_limits"] = energy_limits
     with tempfile.TemporaryDirectory() as d:
-        solver = Solver(Prebuilt(), cfg, echo_details=False, directory=d, prefix="c5",
+        solver = Solver(sample, cfg, echo_details=False, directory=d, prefix="c5",
                         backend={"precision": precision, "batch": n_states})
         (corr_dos, corr_dc), sec = _timed(solver.calc_corr_dc_cond)
-    an = Analyzer(Prebuilt(), cfg, dimension=2)
+    an = Analyzer(sample, cfg, dimension=2)
     energies, dc = an.calc_dc_cond(corr_dos, corr_dc)
     i0 = int(np.argmin(np.abs(energies)))
-    n = ham[0].size - 1
     f2py.set_backend(precision="fp64", batch=16)
     return {"workload": f"c5 graphene {nx}x{nx}, B={b_field:.2f} T (flux h/e per 1024 "
                         f"hexagons), W=1 eV, {n_states} states, corr_dc {precision}",
-            "n_orbitals": int(n), "steps": steps, "n_energies": int(energies.size),
-            "host_build_seconds": t_build, "seconds": sec,
+            "builder": builder, "n_orbitals": int(n), "steps": steps,
+            "n_energies": int(energies.size),
+            "build_seconds": t_build, "seconds": sec,
             "orbital_steps_per_s": n * n_states * steps / sec,
             "sigma_dc_xx_at_E0": float(dc[0, i0]), "sigma_dc_yy_at_E0": float(dc[1, i0]),
             "corr_dos_1": [float(corr_dos[0].real), float(corr_dos[0].imag)]}
@@ -515,6 +527,8 @@ def main(argv=None) -> None:
                     help="override the number of time steps (shorter runs)")
     ap.add_argument("--out", default=None)
     ap.add_argument("--data", default=None, help="c4: npz cache of the generated curves")
+    ap.add_argument("--builder", default="device", choices=["device", "host"],
+                    help="c5: assemble the Hamiltonian on the GPU or on the host")
     args = ap.parse_args(argv)
     for w in args.workloads:
         kw = {}
@@ -523,6 +537,8 @@ def main(argv=None) -> None:
                  {"steps_dos": args.steps, "steps_ac": args.steps}
         if w == "c4" and args.data:
             kw["data"] = args.data
+        if w == "c5":
+            kw["builder"] = args.builder
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
         print(line, flush=True)
