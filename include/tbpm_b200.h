@@ -222,6 +222,86 @@ int tbpm_psi_t(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indpt
                const double* psi0, const int32_t* time_log, int n_time_log, int n_timestep,
                int wfn_chk_step, double wfn_chk_thr, double* psi_t);
 
+/* tbpm_dyn_pol -- replaces tbpm.f90:355-493 (SUBROUTINE tbpm_dyn_pol) as called
+ * from Solver.calc_corr_dyn_pol (tbpm/solver.py:354-390).
+ * site_x/y/z: float64[n_rows] orbital positions (Sample.orb_pos columns);
+ * q_points: float64 [n_q_points][3] (C order); corr: float64 (n_q_points,
+ * n_timestep) Fortran order, corr(q, t) = Im <psi2(t)| exp(i q.r) psi1(t)>
+ * averaged over the states.  The psi2 vectors of a batch are shared by all its
+ * q-points (they do not depend on q). */
+int tbpm_dyn_pol(tbpm_ctx* ctx, const double* bes, int n_bes, double beta, double mu,
+                 const int32_t* indptr, const int32_t* indices, const double* hop,
+                 int64_t n_rows, int64_t nnz, double h_rescale, const double* dx,
+                 const double* dy, const double* site_x, const double* site_y,
+                 const double* site_z, int seed, int n_timestep, int n_ran_samples,
+                 int nr_fermi, double fermi_precision, const double* q_points, int n_q_points,
+                 int rank, int wfn_chk_step, double wfn_chk_thr, double* corr);
+
+/* As tbpm_dyn_pol with caller-supplied initial states (complex128 [n_states][n_rows]). */
+int tbpm_dyn_pol_states(tbpm_ctx* ctx, const double* bes, int n_bes, double beta, double mu,
+                        const int32_t* indptr, const int32_t* indices, const double* hop,
+                        int64_t n_rows, int64_t nnz, const double* site_x,
+                        const double* site_y, const double* site_z, const double* q_points,
+                        int n_q_points, const double* wf0, int n_states, int n_timestep,
+                        int nr_fermi, double fermi_precision, int wfn_chk_step,
+                        double wfn_chk_thr, double* corr);
+
+/* tbpm_eigenstates -- replaces tbpm.f90:721-830 (SUBROUTINE tbpm_eigenstates)
+ * as called from Solver.calc_quasi_eigenstates (tbpm/solver.py:474-507).
+ * wf_qe: float64 (n_energies, n_rows) Fortran order, the sample average of
+ * |QE_i(r)|^2 of the normalised Hanning-windowed quasi-eigenstates. */
+int tbpm_eigenstates(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+                     const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+                     int seed, int n_timestep, int n_ran_samples, double t_step,
+                     const double* energies, int n_energies, int rank, int wfn_chk_step,
+                     double wfn_chk_thr, double* wf_qe);
+
+/* As tbpm_eigenstates with caller-supplied initial states. */
+int tbpm_eigenstates_states(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_t* indptr,
+                            const int32_t* indices, const double* hop, int64_t n_rows,
+                            int64_t nnz, const double* wf0, int n_states, int n_timestep,
+                            double t_step, const double* energies, int n_energies,
+                            int wfn_chk_step, double wfn_chk_thr, double* wf_qe);
+
+/* tbpm_kbdc -- replaces tbpm.f90:836-960 (SUBROUTINE tbpm_kbdc) as called from
+ * Solver.calc_hall_mu (tbpm/solver.py:443-472).  direction 1: J_x, 2: J_y on
+ * the ket side.  mu: complex128 (n_kernel, n_kernel) Fortran order,
+ * mu(m, n) = g_m g_n <T_m(H) J_x psi | J_dir T_n(H) psi> averaged over the
+ * states (g: Jackson kernel).  The n_kernel^2 inner products run as complex
+ * GEMMs (cuBLAS, loaded on first use); memory: (n_kernel + 134) vectors. */
+int tbpm_kbdc(tbpm_ctx* ctx, int seed, const int32_t* indptr, const int32_t* indices,
+              const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+              const double* dx, const double* dy, int n_ran_samples, int n_kernel,
+              int direction, int rank, double* mu);
+
+/* As tbpm_kbdc with caller-supplied initial states. */
+int tbpm_kbdc_states(tbpm_ctx* ctx, const int32_t* indptr, const int32_t* indices,
+                     const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+                     const double* dx, const double* dy, const double* wf0, int n_states,
+                     int n_kernel, int direction, double* mu);
+
+/* Haydock (Lanczos) coefficients of ldos_haydock -- replaces tbpm.f90:963-1026
+ * with propagation.f90:85-155 (SUBROUTINE Haydock_coef), averaged over
+ * n_samples start vectors whose amplitudes on the sites are wf_sites
+ * (complex128 [n_samples][n_sites]).  coefa: complex128[n_depth],
+ * coefb: float64[n_depth].  The Green function and LDOS on the energy grid
+ * (funcs.f90:152-172) are evaluated by the caller. */
+int tbpm_haydock_coef(tbpm_ctx* ctx, const int32_t* indptr, const int32_t* indices,
+                      const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+                      const int32_t* site_indices, int n_sites, const double* wf_sites,
+                      int n_samples, int n_depth, double* coefa, double* coefb);
+
+/* cond_from_trace -- replaces analysis.f90:6-69 (SUBROUTINE cond_from_trace,
+ * with kpm.f90:31-56 get_gamma_mn) as called from Analyzer.calc_hall_cond
+ * (tbpm/analysis.py:513-575).  mu_mn: complex128 (n_kernel, n_kernel) Fortran
+ * order; mu: chemical potentials (eV); cond: float64[n_mu], before the
+ * Analyzer's prefactor.  The n_kernel^2 x (ne_integral-1) trace runs on the
+ * GPU; the final Fermi integral on the host.  fermi_precision and rank are
+ * accepted for the reference's argument list and unused, as there. */
+int tbpm_cond_from_trace(tbpm_ctx* ctx, const double* mu_mn, int n_kernel, const double* mu,
+                         int n_mu, double h_rescale, double beta, int ne_integral,
+                         double fermi_precision, int rank, double* cond);
+
 /* DOS correlations of many uneven realisations packed into one block-diagonal
  * Hamiltonian (a batch of samples; the TBPM loop of tbpm.f90:50-86 run for
  * every realisation at once).  Realisation k owns rows

@@ -608,4 +608,279 @@ int orc_tbpm_psi_t(const double* bes, int n_bes, const int32_t* indptr,
   return ORC_OK;
 }
 
+// funcs.f90:125-149 (density_coef): exp(+-i q.r) per orbital
+static void density_coef(int64_t n, const double* x, const double* y, const double* z,
+                         const double* q, zc* dq, zc* dmq) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double p = q[0] * x[i] + q[1] * y[i] + q[2] * z[i];
+    dq[i] = zmk(std::cos(p), std::sin(p));
+    dmq[i] = zmk(std::cos(p), -std::sin(p));
+  }
+}
+
+// tbpm.f90:355-493 (tbpm_dyn_pol).  q_points: C order [n_q][3].
+// corr: real (n_q, n_timestep) F-order.
+int orc_tbpm_dyn_pol(const double* bes, int n_bes, double beta, double mu,
+                     const int32_t* indptr, const int32_t* indices, const double* hop,
+                     int64_t n, const double* site_x, const double* site_y,
+                     const double* site_z, const double* q_points, int n_q,
+                     const double* wf0_in, int seed, int n_timestep, int n_samples,
+                     int nr_fermi, double fermi_precision, int rank, int chk_step,
+                     double chk_thr, int state_kind, double* corr) {
+  if (n_bes < 3 || n < 1 || n_timestep < 1 || n_samples < 1 || n_q < 1) return ORC_ERR_ARG;
+  for (int64_t i = 0; i < (int64_t)n_q * n_timestep; ++i) corr[i] = 0.0;
+  Csr h{indptr, indices, reinterpret_cast<const zc*>(hop), n};
+  std::vector<double> coef_f(nr_fermi + 1), coef_omf(nr_fermi + 1);
+  const int n_f = orc_fermi_cheb_coef(coef_f.data(), nr_fermi, beta, mu, 0, fermi_precision);
+  const int n_omf =
+      orc_fermi_cheb_coef(coef_omf.data(), nr_fermi, beta, mu, 1, fermi_precision);
+  if (n_f < 3 || n_omf < 3) return ORC_ERR_ARG;
+  std::vector<zc> dq(n), dmq(n), wf0(n), wf1(n), psi1(n), psi2(n), tmp(n), t0(n), t1(n);
+  for (int iq = 0; iq < n_q; ++iq) {
+    density_coef(n, site_x, site_y, site_z, q_points + 3 * iq, dq.data(), dmq.data());
+    for (int s = 1; s <= n_samples; ++s) {
+      if (wf0_in)
+        std::memcpy(wf0.data(), wf0_in + 2 * (int64_t)(s - 1) * n, sizeof(zc) * n);
+      else
+        random_state(wf0.data(), n, (int64_t)seed * (s + rank * n_samples), state_kind);
+      for (int64_t i = 0; i < n; ++i) tmp[i] = zmul(dmq[i], wf0[i]);
+      fermi_op(h, coef_omf.data(), n_omf, tmp.data(), psi1.data(), t0, t1);
+      fermi_op(h, coef_f.data(), n_f, wf0.data(), psi2.data(), t0, t1);
+      for (int64_t i = 0; i < n; ++i) wf1[i] = zmul(dq[i], psi1[i]);
+      corr[iq] += inner_prod(psi2.data(), wf1.data(), n).im / n_samples;
+      const zc norm_ref = inner_prod(psi2.data(), psi2.data(), n);
+      for (int t = 2; t <= n_timestep; ++t) {
+        if (t == chk_step && norm_broken(psi2.data(), n, norm_ref, chk_thr))
+          return ORC_ERR_NORM;
+        cheb_wf_timestep(h, bes, n_bes, psi1.data(), true, tmp.data(), t0, t1);
+        psi1.swap(tmp);
+        cheb_wf_timestep(h, bes, n_bes, psi2.data(), true, tmp.data(), t0, t1);
+        psi2.swap(tmp);
+        for (int64_t i = 0; i < n; ++i) wf1[i] = zmul(dq[i], psi1[i]);
+        corr[iq + (int64_t)n_q * (t - 1)] += inner_prod(psi2.data(), wf1.data(), n).im / n_samples;
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+// tbpm.f90:721-830 (tbpm_eigenstates).  wf_qe: real (n_energies, n) F-order.
+int orc_tbpm_eigenstates(const double* bes, int n_bes, const int32_t* indptr,
+                         const int32_t* indices, const double* hop, int64_t n,
+                         const double* wf0_in, int seed, int n_timestep, int n_samples,
+                         double t_step, const double* energies, int n_en, int rank,
+                         int chk_step, double chk_thr, int state_kind, double* wf_qe) {
+  if (n_bes < 3 || n < 1 || n_timestep < 1 || n_samples < 1 || n_en < 1) return ORC_ERR_ARG;
+  for (int64_t i = 0; i < (int64_t)n_en * n; ++i) wf_qe[i] = 0.0;
+  Csr h{indptr, indices, reinterpret_cast<const zc*>(hop), n};
+  std::vector<zc> wf0(n), wp(n), wm(n), tmp(n), t0(n), t1(n), wfq((size_t)n * n_en);
+  for (int s = 1; s <= n_samples; ++s) {
+    if (wf0_in)
+      std::memcpy(wf0.data(), wf0_in + 2 * (int64_t)(s - 1) * n, sizeof(zc) * n);
+    else
+      random_state(wf0.data(), n, (int64_t)seed * (s + rank * n_samples), state_kind);
+    wp = wf0;
+    wm = wf0;
+    for (int i = 0; i < n_en; ++i)
+      std::memcpy(wfq.data() + (size_t)i * n, wf0.data(), sizeof(zc) * n);
+    const zc norm_ref = inner_prod(wf0.data(), wf0.data(), n);
+    for (int k = 1; k <= n_timestep; ++k) {
+      if (k == chk_step && (norm_broken(wp.data(), n, norm_ref, chk_thr) ||
+                            norm_broken(wm.data(), n, norm_ref, chk_thr)))
+        return ORC_ERR_NORM;
+      cheb_wf_timestep(h, bes, n_bes, wp.data(), true, tmp.data(), t0, t1);
+      wp.swap(tmp);
+      cheb_wf_timestep(h, bes, n_bes, wm.data(), false, tmp.data(), t0, t1);
+      wm.swap(tmp);
+      const double W = 0.5 * (1 + std::cos(kPi * k / n_timestep));  // Hanning window
+      for (int i = 0; i < n_en; ++i) {
+        const double ph = energies[i] * k * t_step;
+        const zc P = zmk(std::cos(ph), std::sin(ph));
+        zc* q = wfq.data() + (size_t)i * n;
+        for (int64_t j = 0; j < n; ++j) {
+          q[j] = zadd(q[j], dmul(W, zmul(P, wp[j])));
+          q[j] = zadd(q[j], dmul(W, zmul(zconj(P), wm[j])));
+        }
+      }
+    }
+    for (int i = 0; i < n_en; ++i) {
+      zc* q = wfq.data() + (size_t)i * n;
+      const double qs = norm_z(q, n);
+      for (int64_t j = 0; j < n; ++j) q[j] = zdivd(q[j], qs);
+      for (int64_t j = 0; j < n; ++j) {
+        const double a = zabs(q[j]);
+        wf_qe[i + (int64_t)n_en * j] += a * a / n_samples;
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+// tbpm.f90:836-960 (tbpm_kbdc).  direction 1: J_x, 2: J_y on the ket side.
+// mu: complex (n_kernel, n_kernel) F-order.
+int orc_tbpm_kbdc(const int32_t* indptr, const int32_t* indices, const double* hop,
+                  int64_t n, int64_t nnz, double h_rescale, const double* dx, const double* dy,
+                  const double* wf0_in, int seed, int n_samples, int n_kernel, int direction,
+                  int rank, int state_kind, double* mu_out) {
+  if (n < 1 || n_samples < 1 || n_kernel < 2 || (direction != 1 && direction != 2))
+    return ORC_ERR_ARG;
+  const zc* hz = reinterpret_cast<const zc*>(hop);
+  zc* mu = reinterpret_cast<zc*>(mu_out);
+  for (int64_t i = 0; i < (int64_t)n_kernel * n_kernel; ++i) mu[i] = zmk(0, 0);
+  std::vector<zc> curx, cury;
+  current_coefficient(hz, dx, nnz, h_rescale, curx);
+  if (direction == 2) current_coefficient(hz, dy, nnz, h_rescale, cury);
+  Csr h{indptr, indices, hz, n}, cx{indptr, indices, curx.data(), n};
+  Csr cy{indptr, indices, direction == 2 ? cury.data() : curx.data(), n};
+  std::vector<double> g(n_kernel);
+  jackson_kernel(g.data(), n_kernel);
+  std::vector<zc> win(n), w0(n), w1(n), w2(n), dk((size_t)n * n_kernel);
+  std::vector<zc> cmu((size_t)n_kernel * n_kernel);
+  auto col = [&](int j) { return dk.data() + (size_t)j * n; };
+  for (int s = 1; s <= n_samples; ++s) {
+    if (wf0_in)
+      std::memcpy(win.data(), wf0_in + 2 * (int64_t)(s - 1) * n, sizeof(zc) * n);
+    else
+      random_state(win.data(), n, (int64_t)seed * (s + rank * n_samples), state_kind);
+    std::memcpy(col(0), win.data(), sizeof(zc) * n);
+    csr_mv(h, col(0), col(1));
+    for (int j = 2; j < n_kernel; ++j) {
+      csr_mv(h, col(j - 1), col(j));
+      zc* y = col(j);
+      const zc* x = col(j - 2);
+      for (int64_t i = 0; i < n; ++i) y[i] = zadd(dmul(-1.0, x[i]), dmul(2.0, y[i]));
+    }
+    const Csr& cj = direction == 1 ? cx : cy;
+    for (int j = 0; j < n_kernel; ++j) {
+      std::memcpy(w0.data(), col(j), sizeof(zc) * n);
+      csr_mv(cj, w0.data(), col(j));
+    }
+    csr_mv(cx, win.data(), w0.data());
+    for (int j = 0; j < n_kernel; ++j) cmu[(size_t)j * n_kernel] = inner_prod(w0.data(), col(j), n);
+    csr_mv(h, w0.data(), w1.data());
+    for (int j = 0; j < n_kernel; ++j)
+      cmu[1 + (size_t)j * n_kernel] = inner_prod(w1.data(), col(j), n);
+    zc* p0 = w0.data();
+    zc* p1 = w1.data();
+    for (int i = 2; i < n_kernel; ++i) {
+      zc* p2 = p0;
+      amxpby_d(2.0, h, p1, -1.0, p0);  // p2 = 2 H p1 - p0, in place of p0
+      for (int j = 0; j < n_kernel; ++j)
+        cmu[i + (size_t)j * n_kernel] = inner_prod(p2, col(j), n);
+      p0 = p1;
+      p1 = p2;
+    }
+    for (int j = 0; j < n_kernel; ++j)
+      for (int i = 0; i < n_kernel; ++i) {
+        const size_t o = i + (size_t)j * n_kernel;
+        mu[o] = zadd(mu[o], zdivd(dmul(g[i] * g[j], cmu[o]), n_samples));
+      }
+  }
+  return ORC_OK;
+}
+
+// propagation.f90:85-155 (Haydock_coef) for one start vector n1 (overwritten).
+static void haydock_coef(const Csr& h, double h_rescale, zc* n1, int n_depth, zc* coefa,
+                         double* coefb) {
+  const int64_t n = h.n;
+  std::vector<zc> n2(n), nbuf(n);
+  amv_d(h_rescale, h, n1, nbuf.data());
+  coefa[0] = inner_prod(n1, nbuf.data(), n);
+  for (int64_t i = 0; i < n; ++i) nbuf[i] = zadd(zmul(zmk(-coefa[0].re, -coefa[0].im), n1[i]), nbuf[i]);
+  coefb[0] = norm_z(nbuf.data(), n);
+  for (int64_t i = 0; i < n; ++i) n2[i] = zdivd(nbuf[i], coefb[0]);
+  zc* p1 = n1;
+  zc* p2 = n2.data();
+  zc* pb = nbuf.data();
+  for (int d = 1; d < n_depth; ++d) {
+    amv_d(h_rescale, h, p2, pb);
+    coefa[d] = inner_prod(p2, pb, n);
+    const zc a = zmk(-coefa[d].re, -coefa[d].im);
+    const double b = -coefb[d - 1];
+    for (int64_t i = 0; i < n; ++i) pb[i] = zadd(zadd(zmul(a, p2[i]), dmul(b, p1[i])), pb[i]);
+    coefb[d] = norm_z(pb, n);
+    for (int64_t i = 0; i < n; ++i) pb[i] = zdivd(pb[i], coefb[d]);
+    zc* sw = p1;
+    p1 = p2;
+    p2 = pb;
+    pb = sw;
+  }
+}
+
+// tbpm.f90:963-1026 (ldos_haydock): sample-averaged Haydock coefficients.
+// wf_sites (optional, complex [n_samples][n_sites]) replaces the random site
+// amplitudes.  coefa: complex[n_depth], coefb: real[n_depth].
+int orc_haydock_coef(const int32_t* site_indices, int n_sites, const int32_t* indptr,
+                     const int32_t* indices, const double* hop, int64_t n, double h_rescale,
+                     const double* wf_sites, int seed, int n_depth, int n_samples,
+                     int state_kind, double* coefa_out, double* coefb) {
+  if (n < 1 || n_sites < 1 || n_depth < 1 || n_samples < 1) return ORC_ERR_ARG;
+  Csr h{indptr, indices, reinterpret_cast<const zc*>(hop), n};
+  zc* ca = reinterpret_cast<zc*>(coefa_out);
+  for (int d = 0; d < n_depth; ++d) {
+    ca[d] = zmk(0, 0);
+    coefb[d] = 0.0;
+  }
+  std::vector<zc> tmp(n_sites), wf0(n), a(n_depth);
+  std::vector<double> b(n_depth);
+  for (int s = 1; s <= n_samples; ++s) {
+    if (wf_sites)
+      std::memcpy(tmp.data(), wf_sites + 2 * (int64_t)(s - 1) * n_sites, sizeof(zc) * n_sites);
+    else
+      random_state(tmp.data(), n_sites, (int64_t)seed * s, state_kind);
+    std::fill(wf0.begin(), wf0.end(), zmk(0, 0));
+    for (int i = 0; i < n_sites; ++i) {
+      if (site_indices[i] < 0 || site_indices[i] >= n) return ORC_ERR_ARG;
+      wf0[site_indices[i]] = tmp[i];
+    }
+    haydock_coef(h, h_rescale, wf0.data(), n_depth, a.data(), b.data());
+    for (int d = 0; d < n_depth; ++d) {
+      ca[d] = zadd(ca[d], zdivd(a[d], n_samples));
+      coefb[d] += b[d] / n_samples;
+    }
+  }
+  return ORC_OK;
+}
+
+// analysis.f90:6-69 (cond_from_trace) with kpm.f90:31-56 (get_gamma_mn) and
+// funcs.f90:36-57 (Fermi_dist).  mu_mn: complex (n_kernel, n_kernel) F-order.
+int orc_cond_from_trace(const double* mu_mn_in, int n_kernel, const double* mu, int n_mu,
+                        double h_rescale, double beta, int ne_integral, double* cond) {
+  if (n_kernel < 1 || ne_integral < 2) return ORC_ERR_ARG;
+  const zc* mu_mn = reinterpret_cast<const zc*>(mu_mn_in);
+  const double dE = kPi / ne_integral;
+  const int ne = ne_integral - 1;
+  std::vector<double> energy(ne), sum_gamma_mu(ne);
+  for (int k = 1; k <= ne; ++k) {
+    energy[k - 1] = k * dE;
+    const double x = energy[k - 1];
+    const double sx = std::sin(x), cx = std::cos(x);
+    double sum = 0.0;
+#pragma omp parallel for reduction(+ : sum) schedule(static)
+    for (int j = 0; j < n_kernel; ++j) {
+      for (int i = 0; i < n_kernel; ++i) {
+        const zc a = zmul(dmul(std::cos(i * x), zmk(cx, -j * sx)),
+                          zmk(std::cos(j * x), std::sin(j * x)));
+        const zc b = zmul(dmul(std::cos(j * x), zmk(cx, i * sx)),
+                          zmk(std::cos(i * x), -std::sin(i * x)));
+        const zc g = zadd(a, b);
+        sum += zmul(g, mu_mn[i + (size_t)n_kernel * j]).re;
+      }
+    }
+    sum_gamma_mu[k - 1] = sum;
+  }
+  for (int i = 0; i < n_mu; ++i) {
+    double dcx = 0.0;
+    for (int k = 0; k < ne; ++k) {
+      const double s = std::sin(energy[k]);
+      const double div = s * s * s;
+      const double en = std::cos(energy[k]) * h_rescale;
+      const double fd = fermi_dist(beta, mu[i], en);
+      dcx += sum_gamma_mu[k] * fd * dE / div;
+    }
+    cond[i] = dcx;
+  }
+  return ORC_OK;
+}
+
 }  // extern "C"

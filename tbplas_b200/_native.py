@@ -43,7 +43,9 @@ EXPORTED_SYMBOLS = (
     "tbpm_dos_segmented", "tbpm_nn_gemm_tn", "tbpm_nn_transpose_bf16", "tbpm_nn_im2col",
     "tbpm_nn_col2im", "tbpm_nn_bias_act", "tbpm_nn_act_backward", "tbpm_nn_colsum",
     "tbpm_nn_mse", "tbpm_nn_adam", "tbpm_nn_cast_bf16", "tbpm_supercell_ham",
-    "tbpm_supercell_csr",
+    "tbpm_supercell_csr", "tbpm_dyn_pol", "tbpm_dyn_pol_states", "tbpm_eigenstates",
+    "tbpm_eigenstates_states", "tbpm_kbdc", "tbpm_kbdc_states", "tbpm_haydock_coef",
+    "tbpm_cond_from_trace",
 )
 
 
@@ -162,6 +164,26 @@ _SIGNATURES = {
     "tbpm_supercell_ham": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,
                                     ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64),
                                     ctypes.POINTER(_c_dbl)]),
+    "tbpm_dyn_pol": (_c_int, [_vp, _vp, _c_int, _c_dbl, _c_dbl, _vp, _vp, _vp, _c_i64, _c_i64,
+                              _c_dbl, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int,
+                              _c_dbl, _vp, _c_int, _c_int, _c_int, _c_dbl, _vp]),
+    "tbpm_dyn_pol_states": (_c_int, [_vp, _vp, _c_int, _c_dbl, _c_dbl, _vp, _vp, _vp, _c_i64,
+                                     _c_i64, _vp, _vp, _vp, _vp, _c_int, _vp, _c_int, _c_int,
+                                     _c_int, _c_dbl, _c_int, _c_dbl, _vp]),
+    "tbpm_eigenstates": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64, _c_int,
+                                  _c_int, _c_int, _c_dbl, _vp, _c_int, _c_int, _c_int, _c_dbl,
+                                  _vp]),
+    "tbpm_eigenstates_states": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64, _vp,
+                                         _c_int, _c_int, _c_dbl, _vp, _c_int, _c_int, _c_dbl,
+                                         _vp]),
+    "tbpm_kbdc": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_i64, _c_i64, _c_dbl, _vp, _vp,
+                           _c_int, _c_int, _c_int, _c_int, _vp]),
+    "tbpm_kbdc_states": (_c_int, [_vp, _vp, _vp, _vp, _c_i64, _c_i64, _c_dbl, _vp, _vp, _vp,
+                                  _c_int, _c_int, _c_int, _vp]),
+    "tbpm_haydock_coef": (_c_int, [_vp, _vp, _vp, _vp, _c_i64, _c_i64, _c_dbl, _vp, _c_int,
+                                   _vp, _c_int, _c_int, _vp, _vp]),
+    "tbpm_cond_from_trace": (_c_int, [_vp, _vp, _c_int, _vp, _c_int, _c_dbl, _c_dbl, _c_int,
+                                      _c_dbl, _c_int, _vp]),
     "tbpm_supercell_csr": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,
                                     ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64),
                                     ctypes.POINTER(_c_dbl), _vp, _vp, _vp, _vp, _vp]),

@@ -39,6 +39,22 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
                        double chk_thr, double* corr, double* corr_per_state);
 void drv_session_advance(tbpm_ctx* c, int n_steps);
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done);
+void drv_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
+                 const double* sx, const double* sy, const double* sz, const double* q_points,
+                 int n_q, const double* wf0, int n_states, int seed, int rank,
+                 int n_ran_samples, int n_timestep, int nr_fermi, double fermi_precision,
+                 int chk_step, double chk_thr, double* corr);
+void drv_eigenstates(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0,
+                     int n_states, int seed, int rank, int n_ran_samples, int n_timestep,
+                     double t_step, const double* energies, int n_energies, int chk_step,
+                     double chk_thr, double* wf_qe);
+void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
+              int n_ran_samples, int n_kernel, int direction, double* mu);
+void drv_haydock(tbpm_ctx* c, const int32_t* sites, int n_sites, const double* wf_sites,
+                 int n_samples, int n_depth, double h_rescale, double* coefa, double* coefb);
+void release_blas(tbpm_ctx* c);
+void drv_cond_from_trace(tbpm_ctx* c, const double* mu_mn, int nk, const double* mu, int n_mu,
+                         double h_rescale, double beta, int ne_integral, double* cond);
 void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
                        int64_t* n_rows, int64_t* nnz, double* rescale);
 void drv_supercell_csr(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
@@ -130,6 +146,7 @@ int tbpm_destroy(tbpm_ctx* c) {
   c->ham.dx.release();
   c->ham.dy.release();
   c->ham.diag.release();
+  tbpm::release_blas(c);
   cudaStreamDestroy(c->stream);
   delete c;
   return TBPM_OK;
@@ -196,6 +213,106 @@ int tbpm_supercell_csr(tbpm_ctx* c, const tbpm_supercell* sc, int layout,
   return guarded(c, [&] {
     tbpm::drv_supercell_csr(c, sc, layout, orb_eng_cutoff, n_rows, nnz, rescale, indptr,
                             indices, hop, dx, dy);
+  });
+}
+
+int tbpm_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
+                 const int32_t* indptr, const int32_t* indices, const double* hop,
+                 int64_t n_rows, int64_t nnz, double h_rescale, const double* dx,
+                 const double* dy, const double* site_x, const double* site_y,
+                 const double* site_z, int seed, int n_timestep, int n_ran_samples,
+                 int nr_fermi, double fermi_precision, const double* q_points, int n_q_points,
+                 int rank, int wfn_chk_step, double wfn_chk_thr, double* corr) {
+  return guarded(c, [&] {
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, dx, dy, h_rescale);
+    tbpm::drv_dyn_pol(c, bes, n_bes, beta, mu, site_x, site_y, site_z, q_points, n_q_points,
+                      nullptr, n_ran_samples, seed, rank, n_ran_samples, n_timestep, nr_fermi,
+                      fermi_precision, wfn_chk_step, wfn_chk_thr, corr);
+  });
+}
+
+int tbpm_dyn_pol_states(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
+                        const int32_t* indptr, const int32_t* indices, const double* hop,
+                        int64_t n_rows, int64_t nnz, const double* site_x,
+                        const double* site_y, const double* site_z, const double* q_points,
+                        int n_q_points, const double* wf0, int n_states, int n_timestep,
+                        int nr_fermi, double fermi_precision, int wfn_chk_step,
+                        double wfn_chk_thr, double* corr) {
+  return guarded(c, [&] {
+    if (!wf0) throw tbpm::Error{TBPM_ERR_ARG, "null initial states"};
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, nullptr, nullptr, 1.0);
+    tbpm::drv_dyn_pol(c, bes, n_bes, beta, mu, site_x, site_y, site_z, q_points, n_q_points,
+                      wf0, n_states, 0, 0, n_states, n_timestep, nr_fermi, fermi_precision,
+                      wfn_chk_step, wfn_chk_thr, corr);
+  });
+}
+
+int tbpm_eigenstates(tbpm_ctx* c, const double* bes, int n_bes, const int32_t* indptr,
+                     const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
+                     int seed, int n_timestep, int n_ran_samples, double t_step,
+                     const double* energies, int n_energies, int rank, int wfn_chk_step,
+                     double wfn_chk_thr, double* wf_qe) {
+  return guarded(c, [&] {
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, nullptr, nullptr, 1.0);
+    tbpm::drv_eigenstates(c, bes, n_bes, nullptr, n_ran_samples, seed, rank, n_ran_samples,
+                          n_timestep, t_step, energies, n_energies, wfn_chk_step, wfn_chk_thr,
+                          wf_qe);
+  });
+}
+
+int tbpm_eigenstates_states(tbpm_ctx* c, const double* bes, int n_bes, const int32_t* indptr,
+                            const int32_t* indices, const double* hop, int64_t n_rows,
+                            int64_t nnz, const double* wf0, int n_states, int n_timestep,
+                            double t_step, const double* energies, int n_energies,
+                            int wfn_chk_step, double wfn_chk_thr, double* wf_qe) {
+  return guarded(c, [&] {
+    if (!wf0) throw tbpm::Error{TBPM_ERR_ARG, "null initial states"};
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, nullptr, nullptr, 1.0);
+    tbpm::drv_eigenstates(c, bes, n_bes, wf0, n_states, 0, 0, n_states, n_timestep, t_step,
+                          energies, n_energies, wfn_chk_step, wfn_chk_thr, wf_qe);
+  });
+}
+
+int tbpm_kbdc(tbpm_ctx* c, int seed, const int32_t* indptr, const int32_t* indices,
+              const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+              const double* dx, const double* dy, int n_ran_samples, int n_kernel,
+              int direction, int rank, double* mu) {
+  return guarded(c, [&] {
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, dx, dy, h_rescale);
+    tbpm::drv_kbdc(c, nullptr, n_ran_samples, seed, rank, n_ran_samples, n_kernel, direction,
+                   mu);
+  });
+}
+
+int tbpm_kbdc_states(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
+                     const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+                     const double* dx, const double* dy, const double* wf0, int n_states,
+                     int n_kernel, int direction, double* mu) {
+  return guarded(c, [&] {
+    if (!wf0) throw tbpm::Error{TBPM_ERR_ARG, "null initial states"};
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, dx, dy, h_rescale);
+    tbpm::drv_kbdc(c, wf0, n_states, 0, 0, n_states, n_kernel, direction, mu);
+  });
+}
+
+int tbpm_haydock_coef(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
+                      const double* hop, int64_t n_rows, int64_t nnz, double h_rescale,
+                      const int32_t* site_indices, int n_sites, const double* wf_sites,
+                      int n_samples, int n_depth, double* coefa, double* coefb) {
+  return guarded(c, [&] {
+    maybe_upload(c, indptr, indices, hop, n_rows, nnz, nullptr, nullptr, h_rescale);
+    tbpm::drv_haydock(c, site_indices, n_sites, wf_sites, n_samples, n_depth, h_rescale, coefa,
+                      coefb);
+  });
+}
+
+int tbpm_cond_from_trace(tbpm_ctx* c, const double* mu_mn, int n_kernel, const double* mu,
+                         int n_mu, double h_rescale, double beta, int ne_integral,
+                         double fermi_precision, int rank, double* cond) {
+  (void)fermi_precision;  // unused by the reference too (its cut-off is commented out)
+  (void)rank;
+  return guarded(c, [&] {
+    tbpm::drv_cond_from_trace(c, mu_mn, n_kernel, mu, n_mu, h_rescale, beta, ne_integral, cond);
   });
 }
 

@@ -22,6 +22,10 @@
 #include "tbpm_dc_kernels.cuh"
 #include "tbpm_seg_kernels.cuh"
 #include "tbpm_kernels.cuh"
+#include "tbpm_more_kernels.cuh"
+
+#include <cublas_v2.h>
+#include <dlfcn.h>
 
 namespace tbpm {
 
@@ -867,12 +871,15 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
 
 // ---- DC -----------------------------------------------------------------------
 
-// One batch of nb states of tbpm_dccond (tbpm.f90:586-698).
+// One batch of nb states of tbpm_dccond (tbpm.f90:586-698), or, with qe_acc
+// set, of tbpm_eigenstates (tbpm.f90:753-813): phase 1 only, then every
+// quasi-eigenstate is normalised and acc[r][i] += |QE_i(r)|^2 / n_avg.
 template <typename R, int V>
 void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int nb,
               const StateKeys* keys, const double* host_wf0, int n_timestep, double t_step,
               const std::vector<double>& en_sel, int chk_step, double chk_thr, int n_avg,
-              int n_energies, double* dos_corr, double* dc_corr) {
+              int n_energies, double* dos_corr, double* dc_corr, double* qe_acc = nullptr,
+              const char* who = "tbpm_dccond") {
   using C = typename Cx<R>::t;
   const Ham& h = c->ham;
   const int64_t n = h.n;
@@ -966,9 +973,32 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       read_out(c, host, (size_t)(chk_step - 1) * ld * 3);
       for (int b = 0; b < ld; ++b) {
         const double nv = host[((size_t)(chk_step - 2) * ld + b) * 3 + 2];
-        if (norm_broken(nv, norm_ref[(size_t)b * 3 + 2], thr)) raise_norm("tbpm_dccond", chk_step);
+        if (norm_broken(nv, norm_ref[(size_t)b * 3 + 2], thr)) raise_norm(who, chk_step);
       }
     }
+  }
+  if (qe_acc) {
+    // tbpm.f90:803-813: QE_i / |QE_i|, then |.|^2 averaged over samples
+    const int n_ib = n_en * nb;
+    const int64_t rpt = std::max<int64_t>(64, n / ((int64_t)kSMs * 8));
+    const int pgrid = (int)((n + rpt - 1) / rpt);
+    ensure_partials(c, (size_t)n_ib * pgrid);
+    c->small.ensure(sizeof(double) * std::max(n_ib, 64));
+    qe_sqnorm_kernel<R><<<pgrid, std::min(256, ((n_ib + 31) / 32) * 32), 0, c->stream>>>(
+        qe, n, rpt, n_ib, c->partials.as<double>());
+    TBPM_CK(cudaGetLastError());
+    reduce_rows_kernel<<<std::min(n_ib, 65535), 256, 0, c->stream>>>(
+        c->partials.as<double>(), pgrid, n_ib, c->small.as<double>());
+    TBPM_CK(cudaGetLastError());
+    const int64_t total = n * n_en;
+    const int grid = (int)std::min<int64_t>(blocks_for(total, 256), (int64_t)kSMs * 32);
+    qe_density_kernel<R><<<grid, 256, 0, c->stream>>>(qe, n, n_en, nb, c->small.as<double>(),
+                                                     1.0 / n_avg, qe_acc);
+    TBPM_CK(cudaGetLastError());
+    c->launches += 3;
+    c->model_bytes += 2.0 * (double)n * n_ib * 2 * sizeof(R) + 2.0 * total * 8;
+    TBPM_CK(cudaStreamSynchronize(c->stream));
+    return;
   }
   read_out(c, host, (size_t)n_timestep * ld * 3);
   for (int b = 0; b < nb; ++b)
@@ -1050,6 +1080,297 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
             dc_corr[d + 1] += vals[o + 1] / a / n_avg;
           }
   }
+}
+
+// ---- dynamical polarisation -------------------------------------------------------
+
+// One batch of nb states and nq q-points of tbpm_dyn_pol (tbpm.f90:436-488).
+// The block holds psi1 for every (q-point, state) and psi2 for every state:
+// psi2 does not depend on q, so it is propagated once for all q-points of the
+// batch instead of once per q-point.
+template <typename R, int V>
+void dynpol_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, int nb,
+                  int nq, const QBlock& qb, const double* sx, const double* sy, const double* sz,
+                  const StateKeys* keys, const double* host_wf0, int n_timestep, int chk_step,
+                  double chk_thr, int n_avg, int q0, int n_q_total, double* corr) {
+  using C = typename Cx<R>::t;
+  const int ld = (nq + 1) * nb;
+  const int tpr = nq * nb;
+  c->graph.reset();
+  ensure_vectors(c, ld, nb);
+  c->out.ensure((size_t)std::max(n_timestep, 1) * tpr * 3 * sizeof(double));
+  auto* A = c->A.as<Pack<R, V>>();
+  auto* X = c->X.as<Pack<R, V>>();
+  auto* Y = c->Y.as<Pack<R, V>>();
+  auto* W = c->wf0.as<Pack<R, V>>();
+  const Ham& h = c->ham;
+  if (keys)
+    gen_states<R, V>(c, *keys, nb, c->opts.state_kind, W);
+  else
+    upload_states<R>(c, host_wf0, nb, nb, 0, W);
+  const int64_t total = h.n * ld;
+  dens_init_kernel<R><<<(int)std::min<int64_t>(blocks_for(total, 256), (int64_t)kSMs * 32), 256,
+                        0, c->stream>>>(reinterpret_cast<const C*>(W), sx, sy, sz, qb, nq, nb,
+                                        h.n, reinterpret_cast<C*>(A));
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+  // Fermi operators (tbpm.f90:458-461): 1-F on every psi1 column, F on psi2
+  enqueue_expansion<R, V>(c, ex_fermi, ld, A, X, Y, nullptr, 0, nullptr, Counters{});
+  const Tile td = pick_tile(c, h.n, tpr, dens_corr_kernel<R>, 3 * sizeof(double));
+  const size_t smem = (size_t)td.threads * 3 * sizeof(double);
+  reset_counters(c, 0);
+  auto dcorr = [&]() {
+    ensure_partials(c, (size_t)tpr * 3 * td.grid);
+    dens_corr_kernel<R><<<td.grid, td.threads, smem, c->stream>>>(
+        reinterpret_cast<const C*>(A), sx, sy, sz, qb, nq, nb, h.n, c->partials.as<double>());
+    TBPM_CK(cudaGetLastError());
+    c->launches++;
+    c->model_bytes += (double)h.n * ld * 2 * sizeof(R) + (double)h.n * 24;
+    launch_finalize(c, td.grid, tpr * 3, counters(c, 0), c->out.as<double>());
+  };
+  dcorr();  // t = 1 (tbpm.f90:463-470); its psi2 norm is the norm reference
+  auto step = [&]() {
+    enqueue_expansion<R, V>(c, ex_time, ld, A, X, Y, nullptr, 0, nullptr, Counters{});
+    dcorr();
+  };
+  auto key = plan_key(c, 5, ld, V, ex_time);
+  key_push(key, nq);
+  key_push(key, sx);
+  for (int k = 0; k < nq; ++k)
+    for (int d = 0; d < 3; ++d) key_push(key, qb.q[k][d]);
+  const double thr = effective_thr(c, chk_thr);
+  std::vector<double> host;
+  int done = 0;
+  const bool check = chk_step >= 2 && chk_step <= n_timestep;
+  if (check) {
+    // tbpm.f90:479: at t == chk_step psi2 has been propagated chk_step-2 times
+    run_steps(c, chk_step - 2, key, step);
+    done = chk_step - 2;
+    read_out(c, host, (size_t)(done + 1) * tpr * 3);
+    for (int b = 0; b < nb; ++b) {
+      const double ref = host[(size_t)b * 3 + 2];
+      const double nv = host[((size_t)done * tpr + b) * 3 + 2];
+      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dyn_pol", chk_step);
+    }
+  }
+  run_steps(c, (n_timestep - 1) - done, key, step);
+  read_out(c, host, (size_t)n_timestep * tpr * 3);
+  for (int k = 0; k < nq; ++k)
+    for (int b = 0; b < nb; ++b)
+      for (int t = 1; t <= n_timestep; ++t)
+        corr[(q0 + k) + (size_t)n_q_total * (t - 1)] +=
+            host[((size_t)(t - 1) * tpr + k * nb + b) * 3 + 1] / n_avg;
+}
+
+// ---- Kubo-Bastin mu_mn ------------------------------------------------------------
+
+// cuBLAS is bound at first use (dlopen), so loading the library does not pull
+// it in for drivers that do not need it.
+struct BlasApi {
+  bool ok = false;
+  decltype(&cublasCreate_v2) create = nullptr;
+  decltype(&cublasSetStream_v2) set_stream = nullptr;
+  decltype(&cublasZgemm_v2) zgemm = nullptr;
+  decltype(&cublasCgemm_v2) cgemm = nullptr;
+  decltype(&cublasDestroy_v2) destroy = nullptr;
+};
+
+const BlasApi& blas_api() {
+  static BlasApi api = [] {
+    BlasApi a;
+    void* lib = dlopen("libcublas.so.12", RTLD_NOW | RTLD_LOCAL);
+    if (!lib) lib = dlopen("libcublas.so", RTLD_NOW | RTLD_LOCAL);
+    if (!lib) return a;
+    a.create = reinterpret_cast<decltype(a.create)>(dlsym(lib, "cublasCreate_v2"));
+    a.set_stream = reinterpret_cast<decltype(a.set_stream)>(dlsym(lib, "cublasSetStream_v2"));
+    a.zgemm = reinterpret_cast<decltype(a.zgemm)>(dlsym(lib, "cublasZgemm_v2"));
+    a.cgemm = reinterpret_cast<decltype(a.cgemm)>(dlsym(lib, "cublasCgemm_v2"));
+    a.destroy = reinterpret_cast<decltype(a.destroy)>(dlsym(lib, "cublasDestroy_v2"));
+    a.ok = a.create && a.set_stream && a.zgemm && a.cgemm && a.destroy;
+    return a;
+  }();
+  return api;
+}
+
+template <typename R>
+struct Blas;
+template <>
+struct Blas<double> {
+  using T = cuDoubleComplex;
+  static cublasStatus_t gemm(cublasHandle_t h, int m, int n, int k, const void* A, int lda,
+                             const void* B, int ldb, void* C, int ldc) {
+    const T one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    return blas_api().zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, n, k, &one, (const T*)A, lda,
+                            (const T*)B, ldb, &zero, (T*)C, ldc);
+  }
+};
+template <>
+struct Blas<float> {
+  using T = cuComplex;
+  static cublasStatus_t gemm(cublasHandle_t h, int m, int n, int k, const void* A, int lda,
+                             const void* B, int ldb, void* C, int ldc) {
+    const T one = make_cuComplex(1.0f, 0.0f), zero = make_cuComplex(0.0f, 0.0f);
+    return blas_api().cgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, n, k, &one, (const T*)A, lda,
+                            (const T*)B, ldb, &zero, (T*)C, ldc);
+  }
+};
+
+// scatter site amplitudes into a zeroed vector (tbpm.f90:1005-1008)
+template <typename R>
+__global__ void scatter_sites_kernel(const int32_t* sites, const double2* vals, int n_sites,
+                                     typename Cx<R>::t* v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_sites) return;
+  typename Cx<R>::t o;
+  o.x = (R)vals[i].x;
+  o.y = (R)vals[i].y;
+  v[sites[i]] = o;
+}
+
+// mu[i + nk*j] += g_i g_j Cs[i + kc*j... ] / n_avg for the rows i0..i0+kc of a chunk
+template <typename R>
+__global__ void mu_accum_kernel(const typename Cx<R>::t* cs, int kc, int nk, int i0,
+                                const double* g, double scale, double2* mu) {
+  const int64_t total = (int64_t)kc * nk;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int ii = (int)(e % kc);
+    const int j = (int)(e / kc);
+    const int i = i0 + ii;
+    const typename Cx<R>::t v = cs[e];
+    const double w = g[i] * g[j];
+    double2& m = mu[(int64_t)i + (int64_t)nk * j];
+    m.x += w * (double)v.x * scale;
+    m.y += w * (double)v.y * scale;
+  }
+}
+
+// One state of tbpm_kbdc (tbpm.f90:898-957).  Q holds J_a T_j(H) psi for all
+// j (N x nk, column-major); the bra vectors T_i(H) J_x psi are generated in
+// chunks of kc columns and contracted with Q by one complex GEMM per chunk:
+// the nk^2 inner products of the reference as a (kc x N) . (N x nk) product.
+template <typename R>
+void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double scale,
+                double2* mu_dev) {
+  using C = typename Cx<R>::t;
+  const Ham& h = c->ham;
+  const int64_t n = h.n;
+  const int kc = std::min(nk, 128);
+  const size_t vb = (size_t)n * sizeof(C);
+  C* Q = c->A.as<C>();
+  C* P = c->X.as<C>();
+  C* ring = c->Y.as<C>();  // 5 vectors: T ring (3) and the P carry (2)
+  C* psi = c->wf0.as<C>();
+  C* cs = reinterpret_cast<C*>(c->qe.as<char>());
+  const int grid = (int)std::min<int64_t>(blocks_for(n, 256), (int64_t)kSMs * 16);
+  const C* diag = h.has_diag ? h.diag.as<C>() : nullptr;
+  const R* dj = direction == 1 ? h.dx.as<R>() : h.dy.as<R>();
+  auto hmv = [&](double alpha, double beta, const C* x, const C* z, C* y) {
+    cheb_vec_kernel<R><<<grid, 256, 0, c->stream>>>(h.indptr.as<int32_t>(),
+                                                   h.indices.as<int32_t>(), h.hop.as<C>(), diag,
+                                                   n, alpha, beta, x, z, y);
+    TBPM_CK(cudaGetLastError());
+    c->launches++;
+  };
+  auto cur = [&](const R* d, const C* x, C* y) {
+    current_vec_kernel<R><<<grid, 256, 0, c->stream>>>(h.indptr.as<int32_t>(),
+                                                      h.indices.as<int32_t>(), h.hop.as<C>(),
+                                                      d, h.rescale, n, x, y);
+    TBPM_CK(cudaGetLastError());
+    c->launches++;
+  };
+  // ket side: Q_j = J_a T_j(H) psi  (tbpm.f90:905-929)
+  C* t[3] = {ring, ring + n, ring + 2 * n};
+  TBPM_CK(cudaMemcpyAsync(t[0], psi, vb, cudaMemcpyDeviceToDevice, c->stream));
+  for (int j = 0; j < nk; ++j) {
+    C* tj = t[j % 3];
+    if (j == 1) hmv(1.0, 0.0, t[0], nullptr, tj);
+    if (j >= 2) hmv(2.0, -1.0, t[(j - 1) % 3], t[(j - 2) % 3], tj);
+    cur(dj, tj, Q + (size_t)j * n);
+  }
+  // bra side in chunks: P_i = T_i(H) J_x psi, then mu[i0:i0+kc, :] += P^H Q
+  C* carry[2] = {ring + 3 * n, ring + 4 * n};
+  cublasHandle_t bh = reinterpret_cast<cublasHandle_t>(c->blas);
+  for (int i0 = 0; i0 < nk; i0 += kc) {
+    const int m = std::min(kc, nk - i0);
+    for (int ii = 0; ii < m; ++ii) {
+      const int i = i0 + ii;
+      C* pi = P + (size_t)ii * n;
+      // the two previous bra vectors: in this chunk or carried from the last one
+      const C* pm1 = ii >= 1 ? P + (size_t)(ii - 1) * n : carry[1];
+      const C* pm2 = ii >= 2 ? P + (size_t)(ii - 2) * n : (ii == 1 ? carry[1] : carry[0]);
+      if (i == 0)
+        cur(h.dx.as<R>(), psi, pi);  // p_0 = J_x psi (tbpm.f90:932)
+      else if (i == 1)
+        hmv(1.0, 0.0, pm1, nullptr, pi);  // p_1 = H p_0 (:938)
+      else
+        hmv(2.0, -1.0, pm1, pm2, pi);  // p_i = 2 H p_i-1 - p_i-2 (:950)
+    }
+    if (Blas<R>::gemm(bh, m, nk, (int)n, P, (int)n, Q, (int)n, cs, m) != CUBLAS_STATUS_SUCCESS)
+      throw Error{TBPM_ERR_CUDA, "complex GEMM of the Kubo-Bastin moments failed"};
+    mu_accum_kernel<R><<<(int)std::min<int64_t>(blocks_for((int64_t)m * nk, 256), 4096), 256, 0,
+                         c->stream>>>(cs, m, nk, i0, g_dev, scale, mu_dev);
+    TBPM_CK(cudaGetLastError());
+    c->launches += 2;
+    // carry the last two bra vectors into the next chunk
+    if (i0 + m < nk) {  // m == kc >= 2 here
+      TBPM_CK(cudaMemcpyAsync(carry[0], P + (size_t)(m - 2) * n, vb, cudaMemcpyDeviceToDevice,
+                              c->stream));
+      TBPM_CK(cudaMemcpyAsync(carry[1], P + (size_t)(m - 1) * n, vb, cudaMemcpyDeviceToDevice,
+                              c->stream));
+    }
+  }
+  c->model_bytes += (double)nk * (2.0 * ((double)(h.n + 1) * 4 + (double)h.nnz * (4 + 2 * sizeof(R))) +
+                                  4.0 * n * sizeof(C)) +
+                    2.0 * (double)nk * n * sizeof(C);
+}
+
+// ---- Haydock recursion ---------------------------------------------------------------
+
+// propagation.f90:85-155 for the start vector already in wf0 (single column);
+// a (complex) and b of every depth are written to sc[0 .. 3*n_depth).
+template <typename R>
+void haydock_state(tbpm_ctx* c, int n_depth, double h_rescale, double* sc) {
+  using C = typename Cx<R>::t;
+  const Ham& h = c->ham;
+  const int64_t n = h.n;
+  const int grid = (int)std::min<int64_t>(blocks_for(n, 256), (int64_t)kSMs * 8);
+  ensure_partials(c, (size_t)2 * grid);
+  double* part = c->partials.as<double>();
+  C* v[3] = {c->wf0.as<C>(), c->X.as<C>(), c->Y.as<C>()};
+  const C* diag = h.has_diag ? h.diag.as<C>() : nullptr;
+  double* a = sc;              // [2 * n_depth]
+  double* b = sc + 2 * n_depth;  // [n_depth]
+  C* p1 = v[0];  // n_i-1 (n1 at depth 0)
+  C* p2 = v[0];  // n_i
+  C* pb = v[1];
+  C* spare = v[2];
+  for (int d = 0; d < n_depth; ++d) {
+    haydock_apply_kernel<R><<<grid, 256, 0, c->stream>>>(h.indptr.as<int32_t>(),
+                                                         h.indices.as<int32_t>(), h.hop.as<C>(),
+                                                         diag, n, h_rescale, p2, pb, part);
+    small_reduce_kernel<<<1, 256, 0, c->stream>>>(part, grid, 2, 0, a + 2 * d);
+    haydock_orth_kernel<R><<<grid, 256, 0, c->stream>>>(n, a + 2 * d,
+                                                        d ? b + d - 1 : nullptr, p2, p1, pb,
+                                                        part);
+    small_reduce_kernel<<<1, 256, 0, c->stream>>>(part, grid, 1, 1, b + d);
+    C* dst = d == 0 ? spare : pb;  // n2 = m2 / b1 into its own vector at depth 0
+    scale_inv_kernel<R><<<grid, 256, 0, c->stream>>>(n, b + d, pb, dst);
+    TBPM_CK(cudaGetLastError());
+    c->launches += 5;
+    if (d == 0) {
+      p1 = v[0];
+      p2 = spare;
+      // pb keeps its buffer
+    } else {
+      C* sw = p1;
+      p1 = p2;
+      p2 = pb;
+      pb = sw;
+    }
+  }
+  c->model_bytes += (double)n_depth * ((double)(h.n + 1) * 4 + (double)h.nnz * (4 + 2 * sizeof(R)) +
+                                       9.0 * n * sizeof(C));
 }
 
 // ---- psi(t) -------------------------------------------------------------------
@@ -1405,6 +1726,293 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
                                        chk_step, chk_thr, n_states, n_energies, dos_corr,
                                        dc_corr);
     });
+  }
+}
+
+void release_blas(tbpm_ctx* c) {
+  if (c->blas && blas_api().ok) blas_api().destroy(reinterpret_cast<cublasHandle_t>(c->blas));
+  c->blas = nullptr;
+}
+
+void drv_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
+                 const double* sx, const double* sy, const double* sz, const double* q_points,
+                 int n_q, const double* wf0, int n_states, int seed, int rank,
+                 int n_ran_samples, int n_timestep, int nr_fermi, double fermi_precision,
+                 int chk_step, double chk_thr, double* corr) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  if (!sx || !sy || !sz) throw Error{TBPM_ERR_ARG, "site coordinates required"};
+  if (!q_points || n_q < 1) throw Error{TBPM_ERR_ARG, "at least one q-point required"};
+  if (!corr) throw Error{TBPM_ERR_ARG, "null output"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  std::fill(corr, corr + (size_t)n_q * n_timestep, 0.0);
+  std::vector<double> cf, comf;
+  const int nf = fermi_coef(nr_fermi, beta, mu, false, fermi_precision, cf);
+  const int nomf = fermi_coef(nr_fermi, beta, mu, true, fermi_precision, comf);
+  if (nf < 3 || nomf < 3) throw Error{TBPM_ERR_ARG, "Fermi expansion shorter than 3 terms"};
+  const Expansion ex_time = time_step_expansion(bes, n_bes);
+  const int64_t n = c->ham.n;
+  DevMem sites;
+  sites.ensure((size_t)n * 3 * sizeof(double));
+  double* dsx = sites.as<double>();
+  TBPM_CK(cudaMemcpyAsync(dsx, sx, n * 8, cudaMemcpyHostToDevice, c->stream));
+  TBPM_CK(cudaMemcpyAsync(dsx + n, sy, n * 8, cudaMemcpyHostToDevice, c->stream));
+  TBPM_CK(cudaMemcpyAsync(dsx + 2 * n, sz, n * 8, cudaMemcpyHostToDevice, c->stream));
+  const int B = std::min(std::min(batch_size(c), n_states), kMaxCols / 2);
+  const int nq_max = std::max(1, kMaxCols / B - 1);
+  for (int q0 = 0; q0 < n_q; q0 += nq_max) {
+    const int nq = std::min(nq_max, n_q - q0);
+    QBlock qb{};
+    for (int k = 0; k < nq; ++k)
+      for (int d = 0; d < 3; ++d) qb.q[k][d] = q_points[3 * (q0 + k) + d];
+    for (int s0 = 0; s0 < n_states; s0 += B) {
+      const int nb = std::min(B, n_states - s0);
+      const int ld = (nq + 1) * nb;
+      unsigned long long set_b = 0;
+      for (int col = nq * nb; col < ld; ++col) set_b |= 1ull << col;
+      const Expansion ex_fermi = fermi_expansion(comf.data(), nomf, cf.data(), nf, set_b);
+      StateKeys keys{};
+      const StateKeys* kp = nullptr;
+      if (!wf0) {
+        keys = make_keys(seed, s0 + 1, nb, rank, n_ran_samples);
+        kp = &keys;
+      }
+      const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * n : nullptr;
+      dispatch(c->ham.prec, pick_V(c->ham.prec, ld, nb, c->opts.vector_width), [&](auto tag) {
+        using P = decltype(tag);
+        dynpol_batch<typename P::Real, P::V>(c, ex_time, ex_fermi, nb, nq, qb, dsx, dsx + n,
+                                             dsx + 2 * n, kp, hw, n_timestep, chk_step, chk_thr,
+                                             n_states, q0, n_q, corr);
+      });
+    }
+  }
+  c->graph.reset();  // the graphs refer to the site buffer of this call
+}
+
+void drv_eigenstates(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0,
+                     int n_states, int seed, int rank, int n_ran_samples, int n_timestep,
+                     double t_step, const double* energies, int n_energies, int chk_step,
+                     double chk_thr, double* wf_qe) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  if (!energies || n_energies < 1) throw Error{TBPM_ERR_ARG, "at least one energy required"};
+  if (!wf_qe) throw Error{TBPM_ERR_ARG, "null output"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  const int64_t n = c->ham.n;
+  const std::vector<double> en_sel(energies, energies + n_energies);
+  const Expansion ex_fwd = time_step_expansion(bes, n_bes);
+  DevMem acc;
+  acc.ensure((size_t)n * n_energies * sizeof(double));
+  TBPM_CK(cudaMemsetAsync(acc.p, 0, (size_t)n * n_energies * sizeof(double), c->stream));
+  int B = std::min(batch_size(c), kMaxCols / 2);
+  {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t cx = 2 * real_size(c->ham.prec);
+      const size_t per_state =
+          (size_t)n * ((size_t)n_energies * cx + (size_t)(kMaxWindow + 4) * 2 * cx);
+      const size_t reserve = (size_t)6 << 30;
+      const size_t budget = free_b > 2 * reserve ? free_b - reserve : free_b / 2;
+      B = std::min(B, (int)std::max<size_t>(1, budget / std::max<size_t>(per_state, 1)));
+    }
+    (void)cudaGetLastError();
+  }
+  for (int s0 = 0; s0 < n_states; s0 += B) {
+    const int nb = std::min(B, n_states - s0);
+    Expansion ex_pm = ex_fwd;
+    for (int b = nb; b < 2 * nb; ++b) ex_pm.neg_mask |= 1ull << b;
+    StateKeys keys{};
+    const StateKeys* kp = nullptr;
+    if (!wf0) {
+      keys = make_keys(seed, s0 + 1, nb, rank, n_ran_samples);
+      kp = &keys;
+    }
+    const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * n : nullptr;
+    dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb, c->opts.vector_width), [&](auto tag) {
+      using P = decltype(tag);
+      dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep, t_step, en_sel,
+                                       chk_step, chk_thr, n_states, n_energies, nullptr,
+                                       nullptr, acc.as<double>(), "tbpm_eigenstates");
+    });
+  }
+  // acc[r][i] is the Fortran (n_energies, n) layout of wf_QE
+  TBPM_CK(cudaMemcpyAsync(wf_qe, acc.p, (size_t)n * n_energies * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+}
+
+void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
+              int n_ran_samples, int n_kernel, int direction, double* mu) {
+  require_ham(c, true);
+  if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
+  if (n_kernel < 2) throw Error{TBPM_ERR_ARG, "n_kernel must be >= 2"};
+  if (direction != 1 && direction != 2)
+    throw Error{TBPM_ERR_ARG, "Error: wrong direction! (1: x, 2: y)"};
+  if (!mu) throw Error{TBPM_ERR_ARG, "null output"};
+  if (c->ham.n > (int64_t)INT32_MAX) throw Error{TBPM_ERR_ARG, "too many orbitals for the GEMM"};
+  const BlasApi& api = blas_api();
+  if (!api.ok) throw Error{TBPM_ERR_CUDA, "libcublas.so.12 could not be loaded"};
+  if (!c->blas) {
+    cublasHandle_t hnd = nullptr;
+    if (api.create(&hnd) != CUBLAS_STATUS_SUCCESS)
+      throw Error{TBPM_ERR_CUDA, "cublasCreate failed"};
+    c->blas = hnd;
+  }
+  api.set_stream(reinterpret_cast<cublasHandle_t>(c->blas), c->stream);
+  c->launches = 0;
+  c->model_bytes = 0;
+  c->graph.reset();
+  c->sess.active = false;
+  const int64_t n = c->ham.n;
+  const size_t cs = 2 * real_size(c->ham.prec);
+  const int kc = std::min(n_kernel, 128);
+  ensure_vectors(c, 1, 1);
+  c->A.ensure((size_t)n * n_kernel * cs);
+  c->X.ensure((size_t)n * kc * cs);
+  c->Y.ensure((size_t)n * 5 * cs);
+  c->qe.ensure((size_t)kc * n_kernel * cs);
+  // kpm.f90:8-29 Jackson kernel, first element halved
+  std::vector<double> g(n_kernel);
+  g[0] = 0.5;
+  const double pi = 3.14159265358979323846;
+  const double q = pi / n_kernel;
+  const double cotq = std::cos(q) / std::sin(q);
+  for (int k = 1; k < n_kernel; ++k)
+    g[k] = ((double)(n_kernel - k) * std::cos(q * k) + cotq * std::sin(q * k)) / n_kernel;
+  DevMem gdev, mdev;
+  gdev.ensure(sizeof(double) * n_kernel);
+  mdev.ensure(sizeof(double2) * (size_t)n_kernel * n_kernel);
+  TBPM_CK(cudaMemcpyAsync(gdev.p, g.data(), sizeof(double) * n_kernel, cudaMemcpyHostToDevice,
+                          c->stream));
+  TBPM_CK(cudaMemsetAsync(mdev.p, 0, sizeof(double2) * (size_t)n_kernel * n_kernel, c->stream));
+  for (int s = 0; s < n_states; ++s) {
+    if (wf0) {
+      if (c->ham.prec == TBPM_PREC_FP64)
+        upload_states<double>(c, wf0 + 2 * (size_t)s * n, 1, 1, 0, c->wf0.p);
+      else
+        upload_states<float>(c, wf0 + 2 * (size_t)s * n, 1, 1, 0, c->wf0.p);
+    } else {
+      const StateKeys keys = make_keys(seed, s + 1, 1, rank, n_ran_samples);
+      if (c->ham.prec == TBPM_PREC_FP64)
+        gen_states<double, 1>(c, keys, 1, c->opts.state_kind, c->wf0.as<Pack<double, 1>>());
+      else
+        gen_states<float, 1>(c, keys, 1, c->opts.state_kind, c->wf0.as<Pack<float, 1>>());
+    }
+    if (c->ham.prec == TBPM_PREC_FP64)
+      kbdc_state<double>(c, n_kernel, direction, gdev.as<double>(), 1.0 / n_states,
+                         mdev.as<double2>());
+    else
+      kbdc_state<float>(c, n_kernel, direction, gdev.as<double>(), 1.0 / n_states,
+                        mdev.as<double2>());
+  }
+  TBPM_CK(cudaMemcpyAsync(mu, mdev.p, sizeof(double2) * (size_t)n_kernel * n_kernel,
+                          cudaMemcpyDeviceToHost, c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+}
+
+void drv_haydock(tbpm_ctx* c, const int32_t* sites, int n_sites, const double* wf_sites,
+                 int n_samples, int n_depth, double h_rescale, double* coefa, double* coefb) {
+  require_ham(c, false);
+  if (!sites || n_sites < 1 || !wf_sites || n_samples < 1)
+    throw Error{TBPM_ERR_ARG, "site indices and site amplitudes required"};
+  if (n_depth < 1) throw Error{TBPM_ERR_ARG, "recursion depth must be >= 1"};
+  if (!coefa || !coefb) throw Error{TBPM_ERR_ARG, "null output"};
+  const int64_t n = c->ham.n;
+  for (int i = 0; i < n_sites; ++i)
+    if (sites[i] < 0 || sites[i] >= n) throw Error{TBPM_ERR_ARG, "site index out of range"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  c->graph.reset();
+  c->sess.active = false;
+  const size_t cs = 2 * real_size(c->ham.prec);
+  c->wf0.ensure((size_t)n * cs);
+  c->X.ensure((size_t)n * cs);
+  c->Y.ensure((size_t)n * cs);
+  DevMem dsites, dvals, sc;
+  dsites.ensure(sizeof(int32_t) * n_sites);
+  dvals.ensure(sizeof(double2) * n_sites);
+  sc.ensure(sizeof(double) * 3 * (size_t)n_depth);
+  TBPM_CK(cudaMemcpyAsync(dsites.p, sites, sizeof(int32_t) * n_sites, cudaMemcpyHostToDevice,
+                          c->stream));
+  std::fill(coefa, coefa + 2 * (size_t)n_depth, 0.0);
+  std::fill(coefb, coefb + n_depth, 0.0);
+  std::vector<double> host(3 * (size_t)n_depth);
+  for (int s = 0; s < n_samples; ++s) {
+    TBPM_CK(cudaMemsetAsync(c->wf0.p, 0, (size_t)n * cs, c->stream));
+    TBPM_CK(cudaMemcpyAsync(dvals.p, wf_sites + 2 * (size_t)s * n_sites,
+                            sizeof(double2) * n_sites, cudaMemcpyHostToDevice, c->stream));
+    const int grid = (n_sites + 255) / 256;
+    if (c->ham.prec == TBPM_PREC_FP64) {
+      scatter_sites_kernel<double><<<grid, 256, 0, c->stream>>>(
+          dsites.as<int32_t>(), dvals.as<double2>(), n_sites, c->wf0.as<double2>());
+      haydock_state<double>(c, n_depth, h_rescale, sc.as<double>());
+    } else {
+      scatter_sites_kernel<float><<<grid, 256, 0, c->stream>>>(
+          dsites.as<int32_t>(), dvals.as<double2>(), n_sites, c->wf0.as<float2>());
+      haydock_state<float>(c, n_depth, h_rescale, sc.as<double>());
+    }
+    TBPM_CK(cudaGetLastError());
+    TBPM_CK(cudaMemcpyAsync(host.data(), sc.p, host.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+    TBPM_CK(cudaStreamSynchronize(c->stream));
+    for (int d = 0; d < n_depth; ++d) {
+      coefa[2 * d] += host[2 * d] / n_samples;
+      coefa[2 * d + 1] += host[2 * d + 1] / n_samples;
+      coefb[d] += host[2 * (size_t)n_depth + d] / n_samples;
+    }
+  }
+}
+
+void drv_cond_from_trace(tbpm_ctx* c, const double* mu_mn, int nk, const double* mu, int n_mu,
+                         double h_rescale, double beta, int ne_integral, double* cond) {
+  if (!mu_mn || nk < 1 || !cond || (n_mu > 0 && !mu)) throw Error{TBPM_ERR_ARG, "bad arguments"};
+  if (ne_integral < 2) throw Error{TBPM_ERR_ARG, "ne_integral must be >= 2"};
+  if ((size_t)nk * 2 * sizeof(double) > 200 * 1024)
+    throw Error{TBPM_ERR_ARG, "n_kernel too large for the trace kernel (max 12800)"};
+  const int ne = ne_integral - 1;
+  DevMem dmu, dsum;
+  dmu.ensure(sizeof(double2) * (size_t)nk * nk);
+  dsum.ensure(sizeof(double) * ne);
+  TBPM_CK(cudaMemcpyAsync(dmu.p, mu_mn, sizeof(double2) * (size_t)nk * nk,
+                          cudaMemcpyHostToDevice, c->stream));
+  const size_t smem = (size_t)nk * 2 * sizeof(double);
+  if (smem > 48 * 1024)
+    TBPM_CK(cudaFuncSetAttribute(gamma_trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  gamma_trace_kernel<<<ne, 256, smem, c->stream>>>(dmu.as<double2>(), nk, ne_integral,
+                                                   dsum.as<double>());
+  TBPM_CK(cudaGetLastError());
+  std::vector<double> sum(ne);
+  TBPM_CK(cudaMemcpyAsync(sum.data(), dsum.p, sizeof(double) * ne, cudaMemcpyDeviceToHost,
+                          c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  // final integral over the Fermi distribution (analysis.f90:55-67)
+  const double pi = 3.14159265358979323846;
+  const double dE = pi / ne_integral;
+  for (int i = 0; i < n_mu; ++i) {
+    double dcx = 0.0;
+    for (int k = 1; k <= ne; ++k) {
+      const double e = k * dE;
+      const double s = std::sin(e);
+      const double div = s * s * s;
+      const double en = std::cos(e) * h_rescale;
+      double fd;
+      if (en >= mu[i]) {
+        const double x = std::exp(beta * (mu[i] - en));
+        fd = x / (1 + x);
+      } else {
+        const double x = std::exp(beta * (en - mu[i]));
+        fd = 1 / (1 + x);
+      }
+      dcx += sum[k - 1] * fd * dE / div;
+    }
+    cond[i] = dcx;
   }
 }
 

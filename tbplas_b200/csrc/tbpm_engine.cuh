@@ -105,4 +105,5 @@ struct tbpm_ctx {
   double model_bytes = 0;
   tbpm::Session sess;
   tbpm::GraphCache graph;
+  void* blas = nullptr;  // cublasHandle_t of the Kubo-Bastin GEMMs (created on first use)
 };

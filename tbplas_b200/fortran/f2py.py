@@ -18,8 +18,10 @@ import numpy as np
 from .. import _native as nat
 
 __all__ = ["tbpm_dos", "tbpm_accond", "tbpm_dccond", "tbpm_psi_t", "tbpm_ldos",
+           "tbpm_dyn_pol", "tbpm_eigenstates", "tbpm_kbdc", "ldos_haydock", "cond_from_trace",
            "tbpm_dos_states", "tbpm_accond_states", "tbpm_dccond_states",
-           "tbpm_dos_segmented", "set_backend", "get_backend"]
+           "tbpm_dyn_pol_states", "tbpm_eigenstates_states", "tbpm_kbdc_states",
+           "haydock_coef", "tbpm_dos_segmented", "set_backend", "get_backend"]
 
 _INT32_MAX = np.iinfo(np.int32).max
 
@@ -281,6 +283,199 @@ def tbpm_psi_t(bes, indptr, indices, hop, psi0, time_log, n_timestep, wfn_chk_st
                 float(wfn_chk_thr), nat.ptr(psi_t))
     return psi_t
 
+
+
+def _sites(site_x, site_y, site_z, n):
+    xs = [nat.as_c(a, np.float64) for a in (site_x, site_y, site_z)]
+    if any(a.size != n for a in xs):
+        raise ValueError("site_x/y/z must have one entry per orbital")
+    return xs
+
+
+def _q_points(q_points) -> np.ndarray:
+    q = nat.as_c(np.atleast_2d(np.asarray(q_points, dtype=np.float64)), np.float64)
+    if q.ndim != 2 or q.shape[1] != 3:
+        raise ValueError("q_points must have shape (n_q_points, 3)")
+    return q
+
+
+def tbpm_dyn_pol(bes, beta, mu, s_indptr, s_indices, s_hop, h_rescale, s_dx, s_dy, s_site_x,
+                 s_site_y, s_site_z, seed, n_timestep, n_ran_samples, nr_fermi,
+                 fermi_precision, q_points, output_filename, rank, wfn_chk_step,
+                 wfn_chk_thr) -> np.ndarray:
+    """Dynamical polarisation correlation function (tbpm.f90:355-493).
+
+    :return: (n_q_points, n_timestep) float64, Fortran order
+    """
+    del output_filename
+    bes = nat.as_c(bes, np.float64)
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    dx, dy = _real(s_dx, nnz), _real(s_dy, nnz)
+    sx, sy, sz = _sites(s_site_x, s_site_y, s_site_z, n)
+    q = _q_points(q_points)
+    corr = np.zeros((q.shape[0], int(n_timestep)), dtype=np.float64, order="F")
+    _say(rank, "Calculating dynamical polarization correlation function.")
+    _ctx().call("tbpm_dyn_pol", nat.ptr(bes), bes.size, float(beta), float(mu), nat.ptr(ip),
+                nat.ptr(ix), nat.ptr(hv), n, nnz, float(h_rescale), nat.ptr(dx), nat.ptr(dy),
+                nat.ptr(sx), nat.ptr(sy), nat.ptr(sz), int(seed), int(n_timestep),
+                int(n_ran_samples), int(nr_fermi), float(fermi_precision), nat.ptr(q),
+                q.shape[0], int(rank), int(wfn_chk_step), float(wfn_chk_thr), nat.ptr(corr))
+    return corr
+
+
+def tbpm_dyn_pol_states(bes, beta, mu, s_indptr, s_indices, s_hop, site_x, site_y, site_z,
+                        q_points, wf0, n_timestep, nr_fermi, fermi_precision, wfn_chk_step,
+                        wfn_chk_thr) -> np.ndarray:
+    """tbpm_dyn_pol with caller-supplied initial states wf0 (n_states, n_orb)."""
+    bes = nat.as_c(bes, np.float64)
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    sx, sy, sz = _sites(site_x, site_y, site_z, n)
+    q = _q_points(q_points)
+    w = nat.as_c(np.atleast_2d(wf0), np.complex128)
+    if w.shape[1] != n:
+        raise ValueError("wf0 must have shape (n_states, n_orbitals)")
+    corr = np.zeros((q.shape[0], int(n_timestep)), dtype=np.float64, order="F")
+    _ctx().call("tbpm_dyn_pol_states", nat.ptr(bes), bes.size, float(beta), float(mu),
+                nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, nat.ptr(sx), nat.ptr(sy),
+                nat.ptr(sz), nat.ptr(q), q.shape[0], nat.ptr(w), w.shape[0], int(n_timestep),
+                int(nr_fermi), float(fermi_precision), int(wfn_chk_step), float(wfn_chk_thr),
+                nat.ptr(corr))
+    return corr
+
+
+def tbpm_eigenstates(bes, s_indptr, s_indices, s_hop, seed, n_timestep, n_ran_samples, t_step,
+                     energies, rank, wfn_chk_step, wfn_chk_thr) -> np.ndarray:
+    """Quasi-eigenstates (tbpm.f90:721-830).
+
+    :return: (n_energies, n_orbitals) float64, Fortran order
+    """
+    bes = nat.as_c(bes, np.float64)
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    en = nat.as_c(energies, np.float64).reshape(-1)
+    out = np.zeros((en.size, n), dtype=np.float64, order="F")
+    _say(rank, "Calculating quasi-eigenstates.")
+    _ctx().call("tbpm_eigenstates", nat.ptr(bes), bes.size, nat.ptr(ip), nat.ptr(ix),
+                nat.ptr(hv), n, nnz, int(seed), int(n_timestep), int(n_ran_samples),
+                float(t_step), nat.ptr(en), en.size, int(rank), int(wfn_chk_step),
+                float(wfn_chk_thr), nat.ptr(out))
+    return out
+
+
+def tbpm_eigenstates_states(bes, s_indptr, s_indices, s_hop, wf0, n_timestep, t_step,
+                            energies, wfn_chk_step, wfn_chk_thr) -> np.ndarray:
+    """tbpm_eigenstates with caller-supplied initial states wf0 (n_states, n_orb)."""
+    bes = nat.as_c(bes, np.float64)
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    en = nat.as_c(energies, np.float64).reshape(-1)
+    w = nat.as_c(np.atleast_2d(wf0), np.complex128)
+    if w.shape[1] != n:
+        raise ValueError("wf0 must have shape (n_states, n_orbitals)")
+    out = np.zeros((en.size, n), dtype=np.float64, order="F")
+    _ctx().call("tbpm_eigenstates_states", nat.ptr(bes), bes.size, nat.ptr(ip), nat.ptr(ix),
+                nat.ptr(hv), n, nnz, nat.ptr(w), w.shape[0], int(n_timestep), float(t_step),
+                nat.ptr(en), en.size, int(wfn_chk_step), float(wfn_chk_thr), nat.ptr(out))
+    return out
+
+
+def tbpm_kbdc(seed, s_indptr, s_indices, s_hop, h_rescale, s_dx, s_dy, n_ran_samples,
+              n_kernel, direction, rank) -> np.ndarray:
+    """Kubo-Bastin moments mu_mn (tbpm.f90:836-960).
+
+    :return: (n_kernel, n_kernel) complex128, Fortran order
+    """
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    dx, dy = _real(s_dx, nnz), _real(s_dy, nnz)
+    mu = np.zeros((int(n_kernel), int(n_kernel)), dtype=np.complex128, order="F")
+    _say(rank, "Calculating Kubo-Bastin moments.")
+    _ctx().call("tbpm_kbdc", int(seed), nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz,
+                float(h_rescale), nat.ptr(dx), nat.ptr(dy), int(n_ran_samples), int(n_kernel),
+                int(direction), int(rank), nat.ptr(mu))
+    return mu
+
+
+def tbpm_kbdc_states(s_indptr, s_indices, s_hop, h_rescale, s_dx, s_dy, wf0, n_kernel,
+                     direction) -> np.ndarray:
+    """tbpm_kbdc with caller-supplied initial states wf0 (n_states, n_orb)."""
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    dx, dy = _real(s_dx, nnz), _real(s_dy, nnz)
+    w = nat.as_c(np.atleast_2d(wf0), np.complex128)
+    if w.shape[1] != n:
+        raise ValueError("wf0 must have shape (n_states, n_orbitals)")
+    mu = np.zeros((int(n_kernel), int(n_kernel)), dtype=np.complex128, order="F")
+    _ctx().call("tbpm_kbdc_states", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz,
+                float(h_rescale), nat.ptr(dx), nat.ptr(dy), nat.ptr(w), w.shape[0],
+                int(n_kernel), int(direction), nat.ptr(mu))
+    return mu
+
+
+def haydock_coef(site_indices, s_indptr, s_indices, s_hop, h_rescale, n_depth, wf_sites):
+    """Sample-averaged Haydock coefficients (propagation.f90:85-155) for start
+    vectors with amplitudes wf_sites (n_samples, n_sites) on site_indices.
+
+    :return: (coefa complex128[n_depth], coefb float64[n_depth])
+    """
+    ip, ix, hv, n, nnz = _csr(s_indptr, s_indices, s_hop)
+    sites = nat.as_c(site_indices, np.int32).reshape(-1)
+    w = nat.as_c(np.atleast_2d(wf_sites), np.complex128)
+    if w.shape[1] != sites.size:
+        raise ValueError("wf_sites must have shape (n_samples, n_sites)")
+    a = np.zeros(int(n_depth), dtype=np.complex128)
+    b = np.zeros(int(n_depth), dtype=np.float64)
+    _ctx().call("tbpm_haydock_coef", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz,
+                float(h_rescale), nat.ptr(sites), sites.size, nat.ptr(w), w.shape[0],
+                int(n_depth), nat.ptr(a), nat.ptr(b))
+    return a, b
+
+
+def green_function(energies, delta, coefa, coefb) -> np.ndarray:
+    """G00(E + i delta) of the Haydock continued fraction (funcs.f90:152-172),
+    for all energies at once."""
+    e = np.asarray(energies, dtype=np.float64) + 1j * float(delta)
+    g = np.zeros(e.shape, dtype=np.complex128)
+    for i in range(len(coefa) - 1, -1, -1):
+        g = 1.0 / (e - coefa[i] - coefb[i] ** 2 * g)
+    return g
+
+
+def ldos_haydock(site_indices, delta, e_range, s_indptr, s_indices, s_hop, h_rescale, seed,
+                 n_depth, n_timestep, n_ran_samples, output_filename):
+    """LDOS by the Haydock recursion (tbpm.f90:963-1026).
+
+    The random start vectors live on site_indices only and are drawn over those
+    sites with the seed rule seed*i_sample (tbpm.f90:1004).
+
+    :return: (energy, ldos), both float64[2*n_timestep+1]
+    """
+    del output_filename
+    sites = np.asarray(site_indices, dtype=np.int64).reshape(-1)
+    n_sites = sites.size
+    if n_sites == 0:
+        raise ValueError("site_indices must not be empty")
+    wf = random_states(n_sites, int(seed), int(n_ran_samples), rank=0,
+                       n_ran_samples=int(n_ran_samples))
+    a, b = haydock_coef(sites, s_indptr, s_indices, s_hop, h_rescale, n_depth, wf)
+    tnr = int(n_timestep)
+    energy = np.array([0.5 * i * e_range / tnr for i in range(-tnr, tnr + 1)])
+    g = green_function(energy, delta, a, b)
+    return energy, -1.0 / np.pi * g.imag
+
+
+def cond_from_trace(mu_mn, mu, h_rescale, beta, ne_integral, fermi_precision,
+                    rank) -> np.ndarray:
+    """Hall conductivity trace of analysis.f90:6-69 (before the Analyzer's
+    prefactor), evaluated on the GPU.
+
+    :return: float64[len(mu)]
+    """
+    m = np.asfortranarray(np.asarray(mu_mn, dtype=np.complex128))
+    if m.ndim != 2 or m.shape[0] != m.shape[1]:
+        raise ValueError("mu_mn must be a square (n_kernel, n_kernel) array")
+    mus = nat.as_c(mu, np.float64).reshape(-1)
+    cond = np.zeros(mus.size, dtype=np.float64)
+    _ctx().call("tbpm_cond_from_trace", m.ctypes.data, m.shape[0], nat.ptr(mus), mus.size,
+                float(h_rescale), float(beta), int(ne_integral), float(fermi_precision),
+                int(rank), nat.ptr(cond))
+    return cond
 
 def random_states(n_orbitals: int, seed: int, n_states: int, rank: int = 0,
                   n_ran_samples: Optional[int] = None, first_sample: int = 1,
