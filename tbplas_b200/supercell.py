@@ -92,9 +92,9 @@ class DeviceSample:
         pos = np.atleast_2d(np.asarray(orb_pos, dtype=np.float64))
         if pos.shape[1] == 2:
             pos = np.hstack([pos, np.zeros((pos.shape[0], 1))])
-        self.orb_pos = np.ascontiguousarray(pos)
+        self.pc_orb_pos = np.ascontiguousarray(pos)
         self.orb_eng = np.ascontiguousarray(orb_eng, dtype=np.float64).reshape(-1)
-        if self.orb_eng.size != self.orb_pos.shape[0]:
+        if self.orb_eng.size != self.pc_orb_pos.shape[0]:
             raise ValueError("one energy per orbital required")
         self.hop_ind = np.ascontiguousarray(hop_ind, dtype=np.int32).reshape(-1, 5)
         self.hop_eng = np.ascontiguousarray(hop_eng, dtype=np.complex128).reshape(-1)
@@ -106,7 +106,7 @@ class DeviceSample:
         self.pbc = tuple(bool(p) for p in pbc)
         v = np.zeros(0, dtype=np.int64) if vac_id_sc is None else np.asarray(vac_id_sc)
         self.vac_id_sc = np.ascontiguousarray(np.unique(v.astype(np.int64)))
-        n_full = int(np.prod(self.dim)) * self.orb_pos.shape[0]
+        n_full = int(np.prod(self.dim)) * self.pc_orb_pos.shape[0]
         self._num_orb = n_full - self.vac_id_sc.size
         self.orb_eng_sc = None
         if orb_eng_sc is not None:
@@ -170,7 +170,30 @@ class DeviceSample:
 
     @property
     def nr_orbitals(self) -> int:
-        return self.orb_pos.shape[0]
+        return self.pc_orb_pos.shape[0]
+
+    @property
+    def orb_pos(self) -> np.ndarray:
+        """Cartesian positions (nm) of the supercell orbitals, (num_orb, 3),
+        as SuperCell.get_orb_pos computes them (cython/super.pyx:569-612 plus
+        the origin, builder/super.py:671-685).  Host arrays; needed by the
+        dynamical polarisation (Sample.orb_pos)."""
+        n_orb = self.pc_orb_pos.shape[0]
+        keep = np.ones(int(np.prod(self.dim)) * n_orb, dtype=bool)
+        keep[self.vac_id_sc] = False
+        g = np.nonzero(keep)[0]
+        cell, o = g // n_orb, g % n_orb
+        ia = cell // (self.dim[1] * self.dim[2])
+        ib = (cell // self.dim[2]) % self.dim[1]
+        ic = cell % self.dim[2]
+        ra = self.pc_orb_pos[o, 0] + ia
+        rb = self.pc_orb_pos[o, 1] + ib
+        rc = self.pc_orb_pos[o, 2] + ic
+        pos = np.empty((g.size, 3))
+        for k in range(3):
+            pos[:, k] = ra * self.lat_vec[0, k] + rb * self.lat_vec[1, k] + \
+                rc * self.lat_vec[2, k]
+        return pos + self.origin
 
     def build_ham_csr(self) -> _ResidentCSR:
         """Handle of the build_ham_csr Hamiltonian, assembled on the GPU when a
@@ -204,8 +227,8 @@ class DeviceSample:
         s = nat.Supercell()
         s.lat_vec = nat.ptr(self.lat_vec)
         s.origin = nat.ptr(self.origin)
-        s.n_orb = self.orb_pos.shape[0]
-        s.orb_pos = nat.ptr(self.orb_pos)
+        s.n_orb = self.pc_orb_pos.shape[0]
+        s.orb_pos = nat.ptr(self.pc_orb_pos)
         s.orb_eng = nat.ptr(self.orb_eng)
         s.n_hop = self.hop_ind.shape[0]
         s.hop_ind = nat.ptr(self.hop_ind) if self.hop_ind.size else None

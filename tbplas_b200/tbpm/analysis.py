@@ -1,10 +1,13 @@
-"""Analyzer: correlation functions -> DOS, AC and DC conductivity.
+"""Analyzer: correlation functions -> DOS, AC/DC/Hall conductivity,
+dynamical polarisation and dielectric function.
 
 Same API and formulas as tbplas/tbpm/analysis.py (window functions :20-51,
-calc_dos :89-143, calc_ac_cond :161-243, calc_dc_cond :375-458,
-calc_diff_coeff :460-511), with the O(nr_time_steps^2) Python loops of the
-reference replaced by numpy array expressions.  Results agree with the
-reference to floating-point summation order.
+calc_dos :89-143, calc_ac_cond :161-243, calc_dyn_pol :245-308, _get_vq
+:310-329, calc_epsilon :331-354, calc_epsilon_q0 :356-373, calc_dc_cond
+:375-458, calc_diff_coeff :460-511, calc_hall_cond :513-575), with the
+O(nr_time_steps^2) Python loops of the reference replaced by numpy array
+expressions and the Kubo-Bastin trace (analysis.f90 cond_from_trace) run on
+the GPU.  Results agree with the reference to floating-point summation order.
 """
 
 from math import cos, exp, pi
@@ -14,6 +17,7 @@ import numpy as np
 from scipy.integrate import cumulative_trapezoid
 from scipy.signal import hilbert
 
+from ..base import EPSILON0
 from ..parallel import MPIEnv
 from .config import Config
 
@@ -199,3 +203,97 @@ class Analyzer(MPIEnv):
             diff_coeff[:, :, 1:] = cumulative_trapezoid(temp, time, axis=2)
         self.bcast(diff_coeff)
         return time, diff_coeff
+
+    def calc_dyn_pol(self, corr_dyn_pol: np.ndarray, window: Callable = window_exp_ten
+                     ) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Dynamical polarisation from its correlation function (analysis.py:245-308).
+
+        :return: (q_points (n_q, 3), omegas (nr_time_steps,), dyn_pol
+            (n_q, nr_time_steps) complex128)
+        """
+        tnr = self._config.generic['nr_time_steps']
+        en_range = self._sample.energy_range
+        t_step = pi / en_range
+        q_points = np.array(self._config.dyn_pol['q_points'], dtype=float)
+        if self._dimension == 2:
+            prefactor = 2. * self._sample.nr_orbitals / (self._sample.area_unit_cell *
+                                                         self._sample.extended)
+        else:
+            prefactor = 2. * self._sample.nr_orbitals / (self._sample.volume_unit_cell *
+                                                         self._sample.extended)
+        omegas = np.array([i * en_range / tnr for i in range(tnr)], dtype=float)
+        dyn_pol = np.zeros((len(q_points), tnr), dtype=complex)
+        if self.is_master:
+            w = _window_values(window, 1, tnr + 1, tnr)
+            k = np.arange(tnr, dtype=float)
+            phi = np.outer(omegas, k * t_step)  # phi[i, k] = k*dt*omega_i
+            e = np.cos(phi) + 1j * np.sin(phi)
+            corr = np.asarray(corr_dyn_pol, dtype=float)[:, :tnr]
+            dyn_pol = prefactor * t_step * ((corr * w[None, :]) @ e.T)
+            if self._config.generic['correct_spin']:
+                dyn_pol = 2. * dyn_pol
+        self.bcast(dyn_pol)
+        return q_points, omegas, dyn_pol
+
+    def _get_vq(self, q_point: np.ndarray) -> float:
+        """Coulomb interaction in momentum space in eV (analysis.py:310-329)."""
+        factor = self._config.dyn_pol['coulomb_constant']
+        back_epsilon = self._config.dyn_pol['background_dielectric_constant']
+        factor /= (EPSILON0 * back_epsilon)
+        q_norm = np.linalg.norm(q_point)
+        if q_norm == 0.0:
+            return 0.0
+        if self._dimension == 2:
+            return factor * 2 * pi / q_norm
+        return factor * 4 * pi / q_norm**2
+
+    def calc_epsilon(self, dyn_pol: np.ndarray) -> np.ndarray:
+        """Dielectric function 1 - V(q) P(q, omega) (analysis.py:331-354)."""
+        tnr = self._config.generic['nr_time_steps']
+        q_points = self._config.dyn_pol['q_points']
+        epsilon = np.zeros((len(q_points), tnr), dtype=complex)
+        if self.is_master:
+            for i, q_point in enumerate(q_points):
+                epsilon[i] = 1 - self._get_vq(q_point) * dyn_pol[i]
+        self.bcast(epsilon)
+        return epsilon
+
+    def calc_epsilon_q0(self, omegas: np.ndarray, ac_cond: np.ndarray) -> np.ndarray:
+        """Dielectric function at q = 0 from the AC conductivity, 3-D only
+        (analysis.py:356-373)."""
+        if self._dimension != 3:
+            raise ValueError(f"Unsupported dimension: {self._dimension}")
+        back_epsilon = self._config.dyn_pol['background_dielectric_constant']
+        prefactor = 4 * pi / (back_epsilon * EPSILON0)
+        return 1 + 1j * prefactor * ac_cond / omegas
+
+    def calc_hall_cond(self, mu_mn: np.ndarray,
+                       unit: str = "h_bar") -> Tuple[np.ndarray, np.ndarray]:
+        """Hall conductivity from the Kubo-Bastin moments (analysis.py:513-575);
+        the trace over Gamma_mn(E) mu_mn runs on the GPU.
+
+        :return: (energies, conductivity) for config.dckb['energies']
+        """
+        from ..fortran import f2py
+        if unit not in ("h_bar", "h"):
+            raise ValueError(f"Illegal unit {unit}")
+        energies = np.array(self._config.dckb['energies'])
+        if self.is_master:
+            prefactor = 16 * self._sample.nr_orbitals / (pi * self._sample.energy_range ** 2)
+            if self._dimension == 2:
+                prefactor /= self._sample.area_unit_cell
+            else:
+                prefactor /= self._sample.volume_unit_cell
+            if unit == "h":
+                prefactor *= (2 * pi)
+            conductivity = f2py.cond_from_trace(
+                mu_mn, self._config.dckb['energies'], self._sample.rescale,
+                self._config.generic['beta'], self._config.dckb['ne_integral'],
+                self._config.generic['Fermi_cheb_precision'], self.rank)
+            conductivity *= prefactor
+            if self._config.generic['correct_spin']:
+                conductivity *= 2
+        else:
+            conductivity = np.zeros(len(energies), dtype=float)
+        self.bcast(conductivity)
+        return energies, conductivity

@@ -251,20 +251,76 @@ class Solver(MPIEnv):
             self._save_data(psi_t, self._output['psi_t'])
         return psi_t
 
-    # -- reference methods outside the GPU hot path ----------------------------
-    def _not_on_path(self, name: str):
-        raise NotImplementedError(
-            f"Solver.{name} is not part of the B200 TBPM path (dynamical polarisation, "
-            f"Kubo-Bastin Hall, quasi-eigenstates and Haydock LDOS are not rebuilt)")
+    def calc_corr_dyn_pol(self) -> np.ndarray:
+        """Dynamical polarisation correlation, (n_q_points, nr_time_steps)
+        float64 (solver.py:354-390)."""
+        self._apply_backend()
+        time_step = 0.5 * self._get_time_step()
+        bessel_series = self._get_bessel_series(time_step)
+        beta_re, mu_re = self._get_beta_mu_re()
+        indptr, indices, hop, dx, dy = self._sample.build_ham_dxy()
+        orb_pos = self._sample.orb_pos
+        site_x, site_y, site_z = orb_pos[:, 0], orb_pos[:, 1], orb_pos[:, 2]
+        num_sample = self._dist_sample()
+        self._echo_time_step_fs(time_step)
+        corr_dyn_pol = f2py.tbpm_dyn_pol(
+            bessel_series, beta_re, mu_re, indptr, indices, hop, self._sample.rescale,
+            dx, dy, site_x, site_y, site_z, self._config.generic['seed'],
+            self._config.generic['nr_time_steps'], num_sample,
+            self._config.generic['nr_Fermi_fft_steps'],
+            self._config.generic['Fermi_cheb_precision'],
+            self._config.dyn_pol['q_points'], self._output['corr_dyn_pol'], self.rank,
+            self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
+        corr_dyn_pol = self.all_average(corr_dyn_pol)
+        self._save_data(corr_dyn_pol, self._output["corr_dyn_pol"])
+        return corr_dyn_pol
 
-    def calc_corr_dyn_pol(self):
-        self._not_on_path("calc_corr_dyn_pol")
+    def calc_hall_mu(self) -> np.ndarray:
+        """Kubo-Bastin moments mu_mn, (n_kernel, n_kernel) complex128
+        (solver.py:443-472)."""
+        self._apply_backend()
+        indptr, indices, hop, dx, dy = self._sample.build_ham_dxy()
+        num_sample = self._dist_sample()
+        mu_mn = f2py.tbpm_kbdc(
+            self._config.generic['seed'], indptr, indices, hop, self._sample.rescale, dx, dy,
+            num_sample, self._config.dckb['n_kernel'], self._config.dckb['direction'],
+            self.rank)
+        mu_mn = self.all_average(mu_mn)
+        self._save_data(mu_mn, self._output['hall_mu'])
+        return mu_mn
 
-    def calc_hall_mu(self):
-        self._not_on_path("calc_hall_mu")
+    def calc_quasi_eigenstates(self, save_data: bool = False) -> np.ndarray:
+        """Quasi-eigenstates, (n_energies, n_orbitals) float64
+        (solver.py:474-507)."""
+        self._apply_backend()
+        time_step = self._get_time_step()
+        bessel_series = self._get_bessel_series(time_step)
+        num_sample = self._dist_sample()
+        self._echo_time_step_fs(time_step)
+        ham_csr = self._sample.build_ham_csr()
+        states = f2py.tbpm_eigenstates(
+            bessel_series, ham_csr.indptr, ham_csr.indices, ham_csr.data,
+            self._config.generic['seed'], self._config.generic['nr_time_steps'], num_sample,
+            time_step, self._config.quasi_eigenstates['energies'], self.rank,
+            self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
+        states = self.all_average(states)
+        if save_data:
+            self._save_data(states, self._output['qe'])
+        return states
 
-    def calc_quasi_eigenstates(self, save_data: bool = False):
-        self._not_on_path("calc_quasi_eigenstates")
-
-    def calc_ldos_haydock(self):
-        self._not_on_path("calc_ldos_haydock")
+    def calc_ldos_haydock(self) -> Tuple[np.ndarray, np.ndarray]:
+        """LDOS by the Haydock recursion: (energies, ldos), both
+        (2*nr_time_steps+1,) float64 (solver.py:509-541)."""
+        if self.size != 1:
+            raise RuntimeError("Using more than 1 mpi process is not allowed"
+                               " for ldos_haydock")
+        self._apply_backend()
+        ham_csr = self._sample.build_ham_csr()
+        energies, ldos = f2py.ldos_haydock(
+            self._config.LDOS['site_indices'], self._config.LDOS['delta'],
+            self._sample.energy_range, ham_csr.indptr, ham_csr.indices, ham_csr.data,
+            self._sample.rescale, self._config.generic['seed'],
+            self._config.LDOS['recursion_depth'], self._config.generic['nr_time_steps'],
+            self._config.generic['nr_random_samples'], self._output['ldos_haydock'])
+        self._save_data(ldos, self._output["ldos_haydock"])
+        return energies, ldos

@@ -169,3 +169,86 @@ def test_cond_from_trace_matches_oracle(sample):
     gpu = f2py.cond_from_trace(mu_mn, mus, sample.rescale, beta, 256, 1e-12, 0)
     ref = oracle.cond_from_trace(mu_mn, mus, sample.rescale, beta, 256)
     assert rel_err(gpu, ref) < FP64_TOL
+
+
+def _solver(sample, cfg, tmp_path, name):
+    return tb.Solver(sample, cfg, echo_details=False, directory=str(tmp_path), prefix=name)
+
+
+def test_solver_methods_end_to_end(sample, tmp_path):
+    """Solver.calc_corr_dyn_pol / calc_quasi_eigenstates / calc_hall_mu /
+    calc_ldos_haydock on the GPU equal the oracle fed with the same seeded
+    states; their output files are written."""
+    cfg = tb.Config()
+    cfg.generic["nr_time_steps"] = 20
+    cfg.generic["nr_random_samples"] = 3
+    cfg.dyn_pol["q_points"] = [[1.0, 0.2, 0.0], [0.3, 1.5, 0.0]]
+    cfg.quasi_eigenstates["energies"] = [-0.2, 0.1]
+    cfg.dckb["n_kernel"] = 32
+    cfg.LDOS["site_indices"] = [5, 9]
+    cfg.LDOS["recursion_depth"] = 25
+    sv = _solver(sample, cfg, tmp_path, "e2e")
+    n = sample.build_ham_csr().shape[0]
+    wf = f2py.random_states(n, 1337, 3)
+    beta, mu = sv._get_beta_mu_re()
+    t = sv._get_time_step()
+    ip, ix, hop, dx, dy = sample.build_ham_dxy()
+    pos = sample.orb_pos
+    dp = sv.calc_corr_dyn_pol()
+    ref = oracle.tbpm_dyn_pol(sv._get_bessel_series(0.5 * t), beta, mu, ip, ix, hop,
+                              pos[:, 0], pos[:, 1], pos[:, 2], cfg.dyn_pol["q_points"], 20,
+                              wf0=wf)
+    assert rel_err(dp, ref) < FP64_TOL
+    assert (tmp_path / "e2e.corr_dyn_pol.npy").exists()
+    h = sample.build_ham_csr()
+    qe = sv.calc_quasi_eigenstates(save_data=True)
+    ref = oracle.tbpm_eigenstates(sv._get_bessel_series(t), h.indptr, h.indices, h.data, 20, t,
+                                  [-0.2, 0.1], wf0=wf)
+    assert rel_err(qe, ref) < FP64_TOL
+    mu_mn = sv.calc_hall_mu()
+    ref = oracle.tbpm_kbdc(ip, ix, hop, sample.rescale, dx, dy, 32, 1, wf0=wf)
+    assert rel_err(mu_mn, ref) < FP64_TOL
+    en, ldos = sv.calc_ldos_haydock()
+    ws = f2py.random_states(2, 1337, 3)
+    ren, rldos = oracle.ldos_haydock([5, 9], cfg.LDOS["delta"], sample.energy_range, h.indptr,
+                                     h.indices, h.data, sample.rescale, 1337, 25, 20, 3,
+                                     wf_sites=ws)
+    assert rel_err(ldos, rldos) < 1e-9
+    an = tb.Analyzer(sample, cfg, dimension=2)
+    q, om, dyn = an.calc_dyn_pol(dp)
+    assert dyn.shape == (2, 20)
+    e, cond = an.calc_hall_cond(mu_mn)
+    assert cond.shape == (len(cfg.dckb["energies"]),) and np.all(np.isfinite(cond))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_analyzer_hall_cond_matches_reference(dim):
+    """calc_hall_cond with the GPU trace against the reference Analyzer's output
+    (tests/golden/reference_drivers.npz)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_drivers.npz"))
+    s = tb.LatticeSample((8, 7))
+    s.orb_eng = s.orb_eng + g["disorder"]
+    s.rescale_ham(9.0)
+    cfg = tb.Config()
+    cfg.dckb["ne_integral"] = 128
+    cfg.dckb["energies"] = [-0.2, -0.1, 0.0, 0.1, 0.2]
+    an = tb.Analyzer(s, cfg, dimension=dim)
+    for unit in ("h_bar", "h"):
+        e, c = an.calc_hall_cond(g["hall/mu_mn_dir2"], unit=unit)
+        assert np.array_equal(e, g[f"analyzer/dim{dim}/hall_energies"])
+        assert rel_err(c, g[f"analyzer/dim{dim}/hall_{unit}"]) < FP64_TOL
+
+
+def test_dyn_pol_on_device_sample_equals_host_route(tmp_path):
+    kw = dict(disorder=0.8, vacancy_rate=0.01, seed=13)
+    dev = tb.make_graphene_device_sample(30, 24, rescale=9.0, **kw)
+    host = tb.make_graphene_sample(30, 24, rescale=9.0, **kw)
+    assert np.array_equal(dev.orb_pos, host.orb_pos)
+    cfg = tb.Config()
+    cfg.generic["nr_time_steps"] = 16
+    cfg.generic["nr_random_samples"] = 2
+    cfg.dyn_pol["q_points"] = [[0.7, 0.7, 0.0]]
+    a = _solver(dev, cfg, tmp_path, "dev").calc_corr_dyn_pol()
+    b = _solver(host, cfg, tmp_path, "host").calc_corr_dyn_pol()
+    assert rel_err(a, b) < 1e-12
