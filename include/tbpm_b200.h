@@ -416,6 +416,20 @@ int tbpm_session_advance(tbpm_ctx* ctx, int n_steps);
  * (either may be NULL).  *n_done receives the number of recorded time rows. */
 int tbpm_session_read(tbpm_ctx* ctx, double* corr, double* norms, int* n_done);
 
+/* Checkpoint support (the reference has no counterpart: its long runs restart
+ * from scratch).  Export copies the session's initial states wf0 and current
+ * states psi (complex128 [n_states][n_rows]) to the host (either may be NULL);
+ * with tbpm_session_read's rows this is everything a DOS run needs to go on. */
+int tbpm_session_export(tbpm_ctx* ctx, double* wf0, double* psi);
+/* Start a DOS session on the uploaded Hamiltonian from such a state: wf0, psi
+ * and the n_done recorded rows (corr complex128 [n_done][n_states], norms
+ * float64 [n_done][n_states]).  With n_done == 0 the session starts from wf0
+ * (row 0 recorded, psi unused), i.e. tbpm_session_dos_begin with given
+ * states.  A resumed run reproduces the uninterrupted one bit for bit. */
+int tbpm_session_dos_resume(tbpm_ctx* ctx, const double* bes, int n_bes, int n_states,
+                            const double* wf0, const double* psi, const double* corr,
+                            const double* norms, int n_done, int n_timestep);
+
 #ifdef __cplusplus
 }
 #endif

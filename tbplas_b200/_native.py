@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "tbpm_nn_mse", "tbpm_nn_adam", "tbpm_nn_cast_bf16", "tbpm_supercell_ham",
     "tbpm_supercell_csr", "tbpm_dyn_pol", "tbpm_dyn_pol_states", "tbpm_eigenstates",
     "tbpm_eigenstates_states", "tbpm_kbdc", "tbpm_kbdc_states", "tbpm_haydock_coef",
-    "tbpm_cond_from_trace",
+    "tbpm_cond_from_trace", "tbpm_session_export", "tbpm_session_dos_resume",
 )
 
 
@@ -182,6 +182,9 @@ _SIGNATURES = {
                                   _c_int, _c_int, _c_int, _vp]),
     "tbpm_haydock_coef": (_c_int, [_vp, _vp, _vp, _vp, _c_i64, _c_i64, _c_dbl, _vp, _c_int,
                                    _vp, _c_int, _c_int, _vp, _vp]),
+    "tbpm_session_export": (_c_int, [_vp, _vp, _vp]),
+    "tbpm_session_dos_resume": (_c_int, [_vp, _vp, _c_int, _c_int, _vp, _vp, _vp, _vp, _c_int,
+                                         _c_int]),
     "tbpm_cond_from_trace": (_c_int, [_vp, _vp, _c_int, _vp, _c_int, _c_dbl, _c_dbl, _c_int,
                                       _c_dbl, _c_int, _vp]),
     "tbpm_supercell_csr": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,

@@ -1,0 +1,173 @@
+"""Checkpoint and resume of long DOS propagations.
+
+The reference's TBPM drivers hold their state inside one Fortran call
+(tbplas/fortran/tbpm.f90:6-93), so a run that is interrupted starts again from
+t = 0.  `dos_checkpointed` runs the same computation as `f2py.tbpm_dos` as a
+device-resident session and, every `every` time steps, writes what the run
+needs to go on to one .npz file:
+
+* the initial states of the current batch of states and their current states
+  (tbpm_session_export), the correlation and norm rows recorded so far
+  (tbpm_session_read);
+* the correlation accumulated over the finished batches, the batch position
+  and a fingerprint of every input (Bessel series, Hamiltonian, seed, sizes,
+  precision, batch width, state distribution).
+
+Called again with the same inputs and path, it resumes from that file
+(tbpm_session_dos_resume) and returns exactly what an uninterrupted run
+returns.  A file whose fingerprint does not match is ignored.  The file is
+written atomically (temporary file + rename) and removed when the run ends.
+"""
+
+import ctypes
+import hashlib
+import os
+import zlib
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _native as nat
+from .fortran import f2py
+
+__all__ = ["dos_checkpointed", "fingerprint"]
+
+
+def _crc(a: np.ndarray) -> int:
+    return zlib.crc32(np.ascontiguousarray(a).view(np.uint8).reshape(-1))
+
+
+def fingerprint(bes, indptr, indices, hop, seed, n_timestep, n_samples, rank,
+                backend: dict) -> str:
+    """Hash of everything the correlation depends on."""
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(bes, dtype=np.float64).tobytes())
+    if hasattr(indptr, "make_resident"):
+        d = indptr.sample
+        for a in (d.lat_vec, d.origin, d.pc_orb_pos, d.orb_eng, d.hop_ind, d.hop_eng,
+                  d.vac_id_sc):
+            h.update(str(_crc(a)).encode())
+        if d.orb_eng_sc is not None:
+            h.update(str(_crc(d.orb_eng_sc)).encode())
+        h.update(repr((d.dim, d.pbc, d.b_field, d.gauge, d.rescale, indptr.layout,
+                       indptr.cutoff)).encode())
+    else:
+        for a in (indptr, indices, hop):
+            a = np.asarray(a)
+            h.update(repr((a.dtype.str, a.shape, _crc(a))).encode())
+    h.update(repr((int(seed), int(n_timestep), int(n_samples), int(rank),
+                   backend["precision"], int(backend["batch"]),
+                   backend["state_kind"])).encode())
+    return h.hexdigest()
+
+
+def _load(path: str, fp: str) -> Optional[dict]:
+    if not os.path.exists(path):
+        return None
+    try:
+        with np.load(path) as z:
+            if str(z["fingerprint"]) != fp:
+                return None
+            return {k: z[k] for k in z.files}
+    except Exception:
+        return None
+
+
+def _save(path: str, **arrays) -> None:
+    tmp = path + ".tmp.npz"
+    np.savez(tmp, **arrays)
+    os.replace(tmp, path)
+
+
+def dos_checkpointed(bes, s_indptr, s_indices, s_hop, seed, n_timestep, n_ran_samples, rank,
+                     wfn_chk_step, wfn_chk_thr, path: str, every: int = 256,
+                     on_checkpoint: Optional[Callable[[int, int], None]] = None) -> np.ndarray:
+    """f2py.tbpm_dos (tbpm.f90:6-93) with a checkpoint file at `path`.
+
+    :param every: time steps between checkpoints
+    :param on_checkpoint: called as on_checkpoint(first_state, rows_done)
+        after every checkpoint write
+    :return: (n_timestep+1,) complex128 correlation, as f2py.tbpm_dos
+    """
+    if every < 1:
+        raise ValueError("every must be >= 1")
+    be = f2py.get_backend()
+    bes = nat.as_c(bes, np.float64)
+    ctx = f2py._ctx()
+    tnr, n_avg = int(n_timestep), int(n_ran_samples)
+    if hasattr(s_indptr, "make_resident"):
+        n, _ = s_indptr.make_resident(ctx)
+    else:
+        ip, ix, hv, n, nnz = f2py._csr(s_indptr, s_indices, s_hop)
+        ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, None, None,
+                 1.0)
+    fp = fingerprint(bes, s_indptr, s_indices, s_hop, seed, tnr, n_avg, rank, be)
+    state = _load(path, fp)
+    B = max(1, min(int(be["batch"]), 64))
+    corr = np.zeros(tnr + 1, dtype=np.complex128)
+    s0, done = 0, 0
+    if state is not None:
+        corr = state["corr"].copy()
+        s0, done = int(state["s0"]), int(state["done"])
+    thr = float(wfn_chk_thr)
+    if be["precision"] == "fp32":
+        thr = max(thr, float(be["fp32_chk_thr"]))
+    while s0 < n_avg:
+        nb = min(B, n_avg - s0)
+        if state is not None and done > 0:
+            wf0 = np.ascontiguousarray(state["wf0"])
+            psi = np.ascontiguousarray(state["psi"])
+            rc = np.ascontiguousarray(state["rows_corr"])
+            rn = np.ascontiguousarray(state["rows_norm"])
+            ctx.call("tbpm_session_dos_resume", nat.ptr(bes), bes.size, nb, nat.ptr(wf0),
+                     nat.ptr(psi), nat.ptr(rc), nat.ptr(rn), done, tnr)
+        else:
+            wf0 = f2py.random_states(n, int(seed), nb, rank=int(rank), n_ran_samples=n_avg,
+                                     first_sample=s0 + 1)
+            ctx.call("tbpm_session_dos_resume", nat.ptr(bes), bes.size, nb, nat.ptr(wf0), None,
+                     None, None, 0, tnr)
+            done = 1
+        state = None
+        rows_c = rows_n = None
+        while done < tnr + 1:
+            k = min(int(every), tnr + 1 - done)
+            ctx.call("tbpm_session_advance", int(k))
+            done += k
+            rows_c = np.zeros((tnr + 1, nb), dtype=np.complex128)
+            rows_n = np.zeros((tnr + 1, nb), dtype=np.float64)
+            got = ctypes.c_int(0)
+            ctx.call("tbpm_session_read", nat.ptr(rows_c), nat.ptr(rows_n), ctypes.byref(got))
+            # tbpm.f90:71-79: at t == wfn_chk_step the state after t-1 steps is
+            # checked against the norm after the first step
+            chk = int(wfn_chk_step)
+            if 2 <= chk <= tnr and done - k <= chk - 1 < done:
+                d = np.abs(rows_n[chk - 1] - rows_n[1])
+                if np.any(~np.isfinite(d)) or np.any(d > thr):
+                    raise nat.NormError(nat.TBPM_ERR_NORM,
+                                        f"tbpm_dos: wave function norm gets broken during "
+                                        f"propagation (time step {chk})")
+            if done < tnr + 1:
+                psi = np.zeros((nb, n), dtype=np.complex128)
+                ctx.call("tbpm_session_export", None, nat.ptr(psi))
+                _save(path, fingerprint=np.array(fp), corr=corr, s0=np.array(s0),
+                      done=np.array(done), wf0=wf0, psi=psi, rows_corr=rows_c[:done],
+                      rows_norm=rows_n[:done])
+                if on_checkpoint is not None:
+                    on_checkpoint(s0, done)
+        # tbpm.f90:58-86: corr(t) += corrval / n_ran_samples, state by state;
+        # real and imaginary parts are divided as reals (a complex division by
+        # (n, 0) rounds differently)
+        acc = corr.view(np.float64)
+        for b in range(nb):
+            acc += np.ascontiguousarray(rows_c[:, b]).view(np.float64) / n_avg
+        s0 += nb
+        done = 0
+        if s0 < n_avg:
+            _save(path, fingerprint=np.array(fp), corr=corr, s0=np.array(s0),
+                  done=np.array(0), wf0=np.zeros(0), psi=np.zeros(0),
+                  rows_corr=np.zeros(0), rows_norm=np.zeros(0))
+            if on_checkpoint is not None:
+                on_checkpoint(s0, 0)
+    if os.path.exists(path):
+        os.remove(path)
+    return corr

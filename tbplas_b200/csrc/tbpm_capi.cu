@@ -39,6 +39,10 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
                        double chk_thr, double* corr, double* corr_per_state);
 void drv_session_advance(tbpm_ctx* c, int n_steps);
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done);
+void drv_session_dos_resume(tbpm_ctx* c, const double* bes, int n_bes, int n_states,
+                            const double* wf0, const double* psi, const double* corr,
+                            const double* norms, int n_done, int n_timestep);
+void drv_session_export(tbpm_ctx* c, double* wf0, double* psi);
 void drv_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
                  const double* sx, const double* sy, const double* sz, const double* q_points,
                  int n_q, const double* wf0, int n_states, int seed, int rank,
@@ -494,6 +498,19 @@ int tbpm_session_advance(tbpm_ctx* c, int n_steps) {
 
 int tbpm_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done) {
   return guarded(c, [&] { tbpm::drv_session_read(c, corr, norms, n_done); });
+}
+
+int tbpm_session_export(tbpm_ctx* c, double* wf0, double* psi) {
+  return guarded(c, [&] { tbpm::drv_session_export(c, wf0, psi); });
+}
+
+int tbpm_session_dos_resume(tbpm_ctx* c, const double* bes, int n_bes, int n_states,
+                            const double* wf0, const double* psi, const double* corr,
+                            const double* norms, int n_done, int n_timestep) {
+  return guarded(c, [&] {
+    tbpm::drv_session_dos_resume(c, bes, n_bes, n_states, wf0, psi, corr, norms, n_done,
+                                 n_timestep);
+  });
 }
 
 }  // extern "C"

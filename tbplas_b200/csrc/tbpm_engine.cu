@@ -622,6 +622,46 @@ void dos_session_begin(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys
   c->sess.ex = ex;
 }
 
+// Resume a DOS session from exported state: initial states wf0, current states
+// psi (complex128 [ns][n]) and the n_done recorded rows (corr complex, norms).
+// n_done == 0 starts a fresh session from the given states (row 0 recorded).
+template <typename R, int V>
+void dos_session_resume(tbpm_ctx* c, const Expansion& ex, int ns, const double* wf0,
+                        const double* psi, const double* corr, const double* norms, int n_done,
+                        int rows_cap) {
+  if (n_done == 0) {
+    dos_session_begin<R, V>(c, ex, ns, nullptr, wf0, rows_cap);
+    return;
+  }
+  c->graph.reset();
+  ensure_vectors(c, ns, ns);
+  c->out.ensure((size_t)rows_cap * ns * 3 * sizeof(double));
+  upload_states<R>(c, wf0, ns, ns, 0, c->wf0.p);
+  upload_states<R>(c, psi, ns, ns, 0, c->A.p);
+  std::vector<double> rows((size_t)n_done * ns * 3);
+  for (int r = 0; r < n_done; ++r)
+    for (int b = 0; b < ns; ++b) {
+      double* v = &rows[((size_t)r * ns + b) * 3];
+      v[0] = corr[2 * ((size_t)r * ns + b)];
+      v[1] = corr[2 * ((size_t)r * ns + b) + 1];
+      v[2] = norms[(size_t)r * ns + b];
+    }
+  TBPM_CK(cudaMemcpyAsync(c->out.p, rows.data(), rows.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, c->stream));
+  // device step counter = next row to record; completion counter = 0
+  const int ctr[2] = {n_done, 0};
+  TBPM_CK(cudaMemcpyAsync(counters(c, 0).step, ctr, sizeof(ctr), cudaMemcpyHostToDevice,
+                          c->stream));
+  TBPM_CK(cudaStreamSynchronize(c->stream));  // host staging buffers go out of scope
+  c->sess.active = true;
+  c->sess.kind = 1;
+  c->sess.ld = ns;
+  c->sess.V = V;
+  c->sess.rows_cap = rows_cap;
+  c->sess.rows_enqueued = n_done;
+  c->sess.ex = ex;
+}
+
 template <typename R, int V>
 void dos_session_advance(tbpm_ctx* c, int n_steps) {
   Session& s = c->sess;
@@ -2138,6 +2178,39 @@ void drv_session_advance(tbpm_ctx* c, int n_steps) {
     using P = decltype(tag);
     dos_session_advance<typename P::Real, P::V>(c, n_steps);
   });
+}
+
+void drv_session_dos_resume(tbpm_ctx* c, const double* bes, int n_bes, int n_states,
+                            const double* wf0, const double* psi, const double* corr,
+                            const double* norms, int n_done, int n_timestep) {
+  require_ham(c, false);
+  if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
+  if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
+  if (!wf0) throw Error{TBPM_ERR_ARG, "null initial states"};
+  if (n_done < 0 || n_done > n_timestep + 1) throw Error{TBPM_ERR_ARG, "bad number of rows"};
+  if (n_done > 0 && (!psi || !corr || !norms)) throw Error{TBPM_ERR_ARG, "null session state"};
+  c->launches = 0;
+  c->model_bytes = 0;
+  const Expansion ex = time_step_expansion(bes, n_bes);
+  dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states, c->opts.vector_width),
+           [&](auto tag) {
+             using P = decltype(tag);
+             dos_session_resume<typename P::Real, P::V>(c, ex, n_states, wf0, psi, corr, norms,
+                                                        n_done, n_timestep + 1);
+           });
+}
+
+void drv_session_export(tbpm_ctx* c, double* wf0, double* psi) {
+  if (!c->sess.active) throw Error{TBPM_ERR_STATE, "no session active"};
+  const int ns = c->sess.ld;
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  if (c->ham.prec == TBPM_PREC_FP64) {
+    if (wf0) download_states<double>(c, c->wf0.p, ns, ns, 0, wf0);
+    if (psi) download_states<double>(c, c->A.p, ns, ns, 0, psi);
+  } else {
+    if (wf0) download_states<float>(c, c->wf0.p, ns, ns, 0, wf0);
+    if (psi) download_states<float>(c, c->A.p, ns, ns, 0, psi);
+  }
 }
 
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done) {

@@ -35,16 +35,22 @@ class Solver(MPIEnv):
     :param backend: GPU backend options (see tbplas_b200.fortran.f2py.set_backend:
         precision 'fp64'/'fp32', batch, device, ...); not part of Config so that
         Config.check_params keeps the reference's key set
+    :param checkpoint: optional {'path': file, 'every': time steps}: calc_corr_dos
+        writes its state to path every `every` steps and resumes from it when
+        called again with the same inputs (tbplas_b200.checkpoint); each rank
+        uses path + '.rank<r>'
     :param kwargs: arguments of set_output
     """
 
     def __init__(self, sample, config: Config, enable_mpi: bool = False,
-                 echo_details: bool = True, backend: dict = None, **kwargs) -> None:
+                 echo_details: bool = True, backend: dict = None, checkpoint: dict = None,
+                 **kwargs) -> None:
         super().__init__(enable_mpi=enable_mpi, echo_details=echo_details)
         self._sample = sample
         self._config = config
         self._config.check_params()
         self._backend = dict(backend or {})
+        self._checkpoint = dict(checkpoint) if checkpoint else None
         self._output = dict()
         self.set_output(**kwargs)
 
@@ -141,11 +147,24 @@ class Solver(MPIEnv):
         ham_csr = self._sample.build_ham_csr()
         num_sample = self._dist_sample()
         self._echo_time_step_fs(time_step)
-        corr_dos = f2py.tbpm_dos(
-            bessel_series, ham_csr.indptr, ham_csr.indices, ham_csr.data,
-            self._config.generic['seed'], self._config.generic['nr_time_steps'],
-            num_sample, self._output['corr_DOS'], self.rank,
-            self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
+        if self._checkpoint:
+            from ..checkpoint import dos_checkpointed
+            path = self._checkpoint["path"]
+            if self.size > 1:
+                path = f"{path}.rank{self.rank}"
+            corr_dos = dos_checkpointed(
+                bessel_series, ham_csr.indptr, ham_csr.indices, ham_csr.data,
+                self._config.generic['seed'], self._config.generic['nr_time_steps'],
+                num_sample, self.rank, self._config.generic['wfn_check_steps'],
+                self._config.generic['wfn_check_thr'], path,
+                every=int(self._checkpoint.get("every", 256)),
+                on_checkpoint=self._checkpoint.get("on_checkpoint"))
+        else:
+            corr_dos = f2py.tbpm_dos(
+                bessel_series, ham_csr.indptr, ham_csr.indices, ham_csr.data,
+                self._config.generic['seed'], self._config.generic['nr_time_steps'],
+                num_sample, self._output['corr_DOS'], self.rank,
+                self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
         corr_dos = self.all_average(corr_dos)
         self._save_data(corr_dos, self._output["corr_DOS"])
         return corr_dos

@@ -97,3 +97,30 @@ def test_device_sample_interface_without_device_work():
         nat._contexts.clear()
         with pytest.raises(nat.TbpmError):
             s.download_ham_csr()
+
+
+def test_checkpoint_fingerprint_tracks_every_input(tmp_path):
+    from tbplas_b200 import checkpoint as ck
+    from tbplas_b200.fortran import f2py
+    s = tb.make_graphene_sample(4, 4, disorder=0.5, rescale=9.0, seed=1)
+    h = s.build_ham_csr()
+    be = f2py.get_backend()
+    base = ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, h.data, 1, 10, 2, 0, be)
+    assert base == ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, h.data, 1, 10, 2, 0, be)
+    other = h.data.copy()
+    other[3] += 1e-12
+    variants = [
+        ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, other, 1, 10, 2, 0, be),
+        ck.fingerprint([0.5, 0.2, 0.11], h.indptr, h.indices, h.data, 1, 10, 2, 0, be),
+        ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, h.data, 2, 10, 2, 0, be),
+        ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, h.data, 1, 11, 2, 0, be),
+        ck.fingerprint([0.5, 0.2, 0.1], h.indptr, h.indices, h.data, 1, 10, 2, 0,
+                       dict(be, precision="fp32")),
+    ]
+    assert len(set(variants + [base])) == len(variants) + 1
+    path = str(tmp_path / "c.npz")
+    ck._save(path, fingerprint=np.array(base), s0=np.array(3))
+    assert int(ck._load(path, base)["s0"]) == 3
+    assert ck._load(path, variants[0]) is None
+    (tmp_path / "bad.npz").write_bytes(b"not a zip")
+    assert ck._load(str(tmp_path / "bad.npz"), base) is None
