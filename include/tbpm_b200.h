@@ -372,10 +372,19 @@ int tbpm_cheb_timestep_noalloc(tbpm_ctx* ctx, const double* bes, int n_bes,
  * activations are channel-last [batch][length][channels]. */
 
 /* C[M,N] = alpha * A[M,K] . B[N,K]^T + beta * C (A, B BF16 with K contiguous,
- * 16-byte aligned rows: K, lda, ldb multiples of 8; C FP32).  Tensor cores
- * (mma.sync m16n8k16 BF16 -> FP32). */
+ * 16-byte aligned rows: K, lda, ldb multiples of 8; C FP32) on the
+ * 5th-generation tensor cores: TMA (128-byte swizzle) into a 4-stage
+ * shared-memory ring, tcgen05.mma (BF16 -> FP32) with the 128 x 128
+ * accumulator in tensor memory, tcgen05.ld epilogue. */
 int tbpm_nn_gemm_tn(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M,
                     int N, int K, float alpha, float beta, void* stream);
+/* The same product through mma.sync m16n8k16 (an independent implementation,
+ * kept to check the tensor-core GEMM). */
+int tbpm_nn_gemm_tn_mma(const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                        int M, int N, int K, float alpha, float beta, void* stream);
+/* 1 in *failed if a bounded wait of the tensor-core GEMM ran out since the
+ * last call (that launch wrote nothing to C); resets the flag.  Synchronous. */
+int tbpm_nn_tc_status(int* failed);
 /* out[c][r] = in[r][c] (BF16) */
 int tbpm_nn_transpose_bf16(const void* in, int rows, int cols, void* out, void* stream);
 /* Xcol[(b*Lout + lo)][j*C + c] = X[b][lo*stride + j - pad][c], zero outside */

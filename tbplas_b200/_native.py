@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "tbpm_supercell_csr", "tbpm_dyn_pol", "tbpm_dyn_pol_states", "tbpm_eigenstates",
     "tbpm_eigenstates_states", "tbpm_kbdc", "tbpm_kbdc_states", "tbpm_haydock_coef",
     "tbpm_cond_from_trace", "tbpm_session_export", "tbpm_session_dos_resume",
+    "tbpm_nn_gemm_tn_mma", "tbpm_nn_tc_status",
 )
 
 
@@ -149,6 +150,9 @@ _SIGNATURES = {
                                     _c_int, _c_int, _c_int, _c_int, _c_int, _c_dbl, _vp, _vp]),
     "tbpm_nn_gemm_tn": (_c_int, [_vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                                  ctypes.c_float, ctypes.c_float, _vp]),
+    "tbpm_nn_gemm_tn_mma": (_c_int, [_vp, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int,
+                                    _c_int, ctypes.c_float, ctypes.c_float, _vp]),
+    "tbpm_nn_tc_status": (_c_int, [ctypes.POINTER(_c_int)]),
     "tbpm_nn_transpose_bf16": (_c_int, [_vp, _c_int, _c_int, _vp, _vp]),
     "tbpm_nn_im2col": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int,
                                 _vp, _vp]),

@@ -3,12 +3,14 @@
 // the caller owns all buffers and the stream.
 //
 //  gemm_tn_bf16_kernel  C[M,N] = alpha * A[M,K] . B[N,K]^T + beta * C  (A, B
-//                       BF16 with K contiguous, C FP32); tensor cores through
-//                       mma.sync m16n8k16 (BF16 in, FP32 accumulate), 128x128x32
-//                       block tiles, cp.async double buffering, ldmatrix
-//                       fragments.  Every dense/convolution product of the
-//                       network (forward, data gradient, weight gradient) is
-//                       this GEMM after an im2col or a transpose.
+//                       BF16 with K contiguous, C FP32) through mma.sync
+//                       m16n8k16, 128x128x32 block tiles, cp.async double
+//                       buffering, ldmatrix fragments: tbpm_nn_gemm_tn_mma, an
+//                       independent implementation kept to check the tcgen05
+//                       GEMM (tbpm_nn_tc.cu) that the network uses.  Every
+//                       dense/convolution product of the network (forward, data
+//                       gradient, weight gradient) is this GEMM after an im2col
+//                       or a transpose.
 //  im2col / col2im      1-D convolution <-> GEMM reshaping, channel-last [B][L][C]
 //  bias_act / act_back  bias + GELU (exact erf form) and its derivative
 //  colsum, mse, adam, cast, transpose
@@ -305,8 +307,8 @@ int status(cudaError_t e) {
 
 extern "C" {
 
-int tbpm_nn_gemm_tn(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M,
-                    int N, int K, float alpha, float beta, void* stream) {
+int tbpm_nn_gemm_tn_mma(const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                        int M, int N, int K, float alpha, float beta, void* stream) {
   if (!A || !B || !C || M < 1 || N < 1 || K < 1 || K % 8 || lda % 8 || ldb % 8 || lda < K ||
       ldb < K || ldc < N)
     return TBPM_ERR_ARG;
