@@ -334,3 +334,43 @@ def dos_l1(corr: np.ndarray, corr_ref: np.ndarray, energy_range: float) -> float
         d = np.interp(e_ref, e, d)
         d /= np.sum(d) * (e_ref[1] - e_ref[0])
     return float(np.sum(np.abs(d - d_ref)) * (e_ref[1] - e_ref[0]))
+
+
+def time_gemm(m: int, n: int, k: int, reps: int = 10, warmup: int = 3) -> Dict[str, float]:
+    """Time the network's tensor-core GEMM (tbpm_nn_gemm_tn, tcgen05) and the
+    mma.sync GEMM on random BF16 operands of shape (m, k) x (n, k)^T with CUDA
+    events; returns milliseconds and TF/s of each."""
+    import torch
+    lib = nat.load_library()
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    a = torch.randn(m, k, device="cuda").to(torch.bfloat16)
+    b = torch.randn(n, k, device="cuda").to(torch.bfloat16)
+    c = torch.zeros(m, n, device="cuda")
+    out: Dict[str, float] = {"m": m, "n": n, "k": k}
+    for name, fn in (("tcgen05", lib.tbpm_nn_gemm_tn), ("mma_sync", lib.tbpm_nn_gemm_tn_mma)):
+        for _ in range(warmup):
+            fn(a.data_ptr(), k, b.data_ptr(), k, c.data_ptr(), n, m, n, k, 1.0, 0.0, s)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn(a.data_ptr(), k, b.data_ptr(), k, c.data_ptr(), n, m, n, k, 1.0, 0.0, s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(reps, 1)
+        out[name + "_ms"] = ms
+        out[name + "_tflops"] = 2.0 * m * n * k / ms / 1e9
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="time the tail network's GEMM kernels")
+    ap.add_argument("--shape", type=int, nargs=3, default=[4096, 4096, 4096],
+                    metavar=("M", "N", "K"))
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    args = ap.parse_args()
+    print(json.dumps(time_gemm(*args.shape, reps=args.reps, warmup=args.warmup)))
