@@ -331,6 +331,7 @@ int tbpm_ham_release(tbpm_ctx* c) {
     c->ham.dx.release();
     c->ham.dy.release();
     c->ham.diag.release();
+    c->raw.release();
     c->ham.has_diag = false;
     c->ham.n = 0;
     c->ham.nnz = 0;

@@ -101,6 +101,7 @@ struct tbpm_ctx {
   std::string err;
   tbpm::Ham ham;
   tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef, seg;
+  tbpm::DevMem raw;  // device copy of an uploaded host CSR, kept for the next upload
   int64_t launches = 0;
   double model_bytes = 0;
   tbpm::Session sess;

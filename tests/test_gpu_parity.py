@@ -203,6 +203,44 @@ def test_invalid_csr_rejected_before_launch(dos_bes):
         f2py.tbpm_dos_states(dos_bes, ip, ix, hv, unit_states(1, 2), 4, 128, 1e-9)
 
 
+@pytest.mark.parametrize("indptr,indices", [([0, 3, 2], [0, 1, 1]),      # indptr decreases
+                                            ([0, 1, 2], [0, -1]),         # negative column
+                                            ([0, 2, 3], [0, 1, 2])])      # column == n
+def test_invalid_csr_variants_rejected(dos_bes, indptr, indices):
+    ip = np.array(indptr, dtype=np.int32)
+    ix = np.array(indices, dtype=np.int32)
+    hv = np.ones(ix.size, dtype=np.complex128)
+    with pytest.raises(ValueError):
+        f2py.tbpm_dos_states(dos_bes, ip, ix, hv, unit_states(1, 2), 4, 128, 1e-9)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", 2e-5)])
+def test_repeated_and_unsorted_diagonal_entries(graphene_small, dos_bes, prec, tol):
+    """Rows with the diagonal split into two entries, placed anywhere in the
+    row: the upload sums them into D; the oracle multiplies them as given."""
+    h = graphene_small.build_ham_csr()
+    n = h.shape[0]
+    rows, cols, vals = [], [], []
+    for r in range(n):
+        a, b = h.indptr[r], h.indptr[r + 1]
+        c, v = list(h.indices[a:b]), list(h.data[a:b])
+        if r % 3 == 0:
+            c = [r] + c + [r]
+            v = [0.01 + 0.002j] + v + [-0.03 + 0j]
+        rows += [r] * len(c)
+        cols += c
+        vals += v
+    ip = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(np.bincount(rows, minlength=n), out=ip[1:])
+    ix = np.array(cols, dtype=np.int32)
+    hv = np.array(vals, dtype=np.complex128)
+    wf0 = unit_states(3, n, seed=21)
+    ref = oracle.tbpm_dos(dos_bes, ip, ix, hv, 24, wf0=wf0)
+    f2py.set_backend(precision=prec)
+    got = f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0, 24, 128, 1e-9)
+    assert rel_err(got, ref) < tol
+
+
 @pytest.mark.parametrize("n_states", [4, 3])
 def test_dos_fp32_error_bounds(graphene_small, dos_bes, n_states):
     ip, ix, hv = _csr(graphene_small)
