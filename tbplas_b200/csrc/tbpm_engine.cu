@@ -914,6 +914,17 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
 // One batch of nb states of tbpm_dccond (tbpm.f90:586-698), or, with qe_acc
 // set, of tbpm_eigenstates (tbpm.f90:753-813): phase 1 only, then every
 // quasi-eigenstate is normalised and acc[r][i] += |QE_i(r)|^2 / n_avg.
+// qe_accum_kernel may need more than the default 48 KB of dynamic shared
+// memory (many energies per block when nb is small).
+template <typename R>
+void qe_smem_attr(size_t bytes) {
+  static size_t granted = 48 * 1024;
+  if (bytes <= granted) return;
+  TBPM_CK(cudaFuncSetAttribute(qe_accum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bytes));
+  granted = bytes;
+}
+
 template <typename R, int V>
 void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int nb,
               const StateKeys* keys, const double* host_wf0, int n_timestep, double t_step,
@@ -991,8 +1002,13 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       StatePtrs<R> win{};
       for (int tau = 0; tau < len; ++tau) win.p[tau] = reinterpret_cast<const C*>(slot(tau));
       const int64_t total = n * n_en * nb;
-      const int grid = (int)std::min<int64_t>(blocks_for(total, 256), (int64_t)kSMs * 64);
-      qe_accum_kernel<R><<<grid, 256, 0, c->stream>>>(qe, n, n_en, nb, win, len,
+      const int qthreads = std::min(256, ((n_en * nb + 31) / 32) * 32);
+      const int n_chunks = (n_en * nb + qthreads - 1) / qthreads;
+      const int64_t tiles = (n + qe_tile_rows(nb) - 1) / qe_tile_rows(nb);
+      const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)kSMs * 8), (unsigned)n_chunks);
+      const size_t qsmem = qe_accum_smem(n_en, nb, qthreads);
+      qe_smem_attr<R>(qsmem);
+      qe_accum_kernel<R><<<grid, qthreads, qsmem, c->stream>>>(qe, n, n_en, nb, win, len,
                                                         c->coef.as<double2>(),
                                                         first_window ? 1 : 0,
                                                         reinterpret_cast<const C*>(W));
@@ -1052,11 +1068,13 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   int64_t rows_per_tile = std::max<int64_t>(64, n / ((int64_t)kSMs * 8));
   const int pgrid = (int)((n + rows_per_tile - 1) / rows_per_tile);
   const int pthreads = std::min(256, ((n_ib + 31) / 32) * 32);
+  const dim3 pgrid2((unsigned)pgrid, (unsigned)((n_ib + pthreads - 1) / pthreads));
+  const size_t psmem = qe_project_smem(nb);
   // |<wf0|QE_i>| per (energy, state)
   ensure_partials(c, (size_t)2 * n_ib * pgrid);
   c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
-  qe_project_kernel<R><<<pgrid, pthreads, 0, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
-                                                          StatePtrs<R>{}, 1, 1,
+  qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
+                                                               StatePtrs<R>{}, 1, 1,
                                                           reinterpret_cast<const C*>(W),
                                                           c->partials.as<double>());
   TBPM_CK(cudaGetLastError());
@@ -1094,9 +1112,9 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       c->launches++;
       u.p[tau] = us;
     }
-    qe_project_kernel<R><<<pgrid, pthreads, 0, c->stream>>>(qe, n, rows_per_tile, n_en, nb, u,
-                                                            len, 0, nullptr,
-                                                            c->partials.as<double>());
+    qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(qe, n, rows_per_tile, n_en,
+                                                                 nb, u, len, 0, nullptr,
+                                                                 c->partials.as<double>());
     TBPM_CK(cudaGetLastError());
     const int64_t n_vals = (int64_t)2 * len * 2 * n_ib;
     reduce_rows_kernel<<<(int)std::min<int64_t>(n_vals, 65535), 256, 0, c->stream>>>(

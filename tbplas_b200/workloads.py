@@ -529,6 +529,8 @@ def main(argv=None) -> None:
     ap.add_argument("--data", default=None, help="c4: npz cache of the generated curves")
     ap.add_argument("--builder", default="device", choices=["device", "host"],
                     help="c5: assemble the Hamiltonian on the GPU or on the host")
+    ap.add_argument("--nx", type=int, default=None,
+                    help="c5: cells per side (default 4096)")
     args = ap.parse_args(argv)
     for w in args.workloads:
         kw = {}
@@ -539,6 +541,8 @@ def main(argv=None) -> None:
             kw["data"] = args.data
         if w == "c5":
             kw["builder"] = args.builder
+            if args.nx:
+                kw["nx"] = args.nx
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
         print(line, flush=True)
