@@ -25,185 +25,336 @@ struct StatePtrs {
   const typename Cx<R>::t* p[kMaxWindow];
 };
 
-// Rows of the window states staged per pass of the QE kernels.
-__host__ __device__ constexpr int qe_tile_rows(int nb) { return nb >= 32 ? 1 : 32 / nb; }
+// ---- quasi-eigenstate kernels: cp.async double-buffered row tiles -----------
+//
+// Both QE kernels walk tiles of qe_tile_rows rows.  While a block works on tile
+// j, the raw values of tile j+1 (window states, and the block's slice of QE)
+// are on their way into shared memory (cp.async, no registers held); a short
+// pass converts each staged value to double once; the tile's arithmetic then
+// reads shared memory only.  Two barriers per tile.
 
-// Shared memory of qe_accum_kernel for nb states and `threads` elements per block.
-__host__ __device__ constexpr size_t qe_accum_smem(int n_en, int nb, int threads) {
-  // a chunk of `threads` consecutive elements spans at most threads / nb + 2 energies
-  return sizeof(double2) *
-         ((size_t)kMaxWindow * (size_t)(n_en < threads / nb + 2 ? n_en : threads / nb + 2) +
-          (size_t)qe_tile_rows(nb) * kMaxWindow * 2 * nb);
+#ifndef TBPM_QE_MINB_A
+#define TBPM_QE_MINB_A 2
+#endif
+#ifndef TBPM_QE_MINB_P
+#define TBPM_QE_MINB_P 2
+#endif
+#ifndef TBPM_QE_ROWS_A
+#define TBPM_QE_ROWS_A 4
+#endif
+// rows per tile of qe_project_kernel, and of qe_accum_kernel (fewer: its tile
+// holds 16 window states)
+template <typename R>
+__host__ __device__ constexpr int qe_tile_rows(int nb) {
+  return nb >= 64 ? 1 : (64 / nb < 8 ? 64 / nb : 8);
+}
+template <typename R>
+__host__ __device__ constexpr int qe_accum_rows(int nb) {
+  return nb >= 64 ? 1 : (64 / nb < TBPM_QE_ROWS_A ? 64 / nb : TBPM_QE_ROWS_A);
+}
+
+// One complex value into shared memory, asynchronously.
+template <typename C>
+__device__ __forceinline__ void qe_cp_async(C* dst, const C* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(C) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void qe_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void qe_cp_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Energies per thread of the QE kernels: a thread updates (or projects) the
+// elements of kQeG energies for one state b, so every staged window / u value
+// it reads from shared memory serves kQeG elements.
+constexpr int kQeG = 2;
+
+// Threads per block of qe_accum_kernel: a multiple of nb (so that the kQeG
+// elements of a thread share their state b), at most 256.
+__host__ __device__ constexpr int qe_accum_threads(int n_en, int nb) {
+  return nb * ((n_en + kQeG - 1) / kQeG < 256 / nb ? (n_en + kQeG - 1) / kQeG : 256 / nb);
+}
+// Threads per block of qe_project_kernel (K threads per element: one per k).
+__host__ __device__ constexpr int qe_project_threads(int n_en, int nb, int K) {
+  return K * nb *
+         ((n_en + kQeG - 1) / kQeG < 256 / (K * nb) ? (n_en + kQeG - 1) / kQeG : 256 / (K * nb));
+}
+
+// Shared memory of qe_accum_kernel.
+template <typename R>
+__host__ __device__ constexpr size_t qe_accum_smem(int n_en, int nb) {
+  return (size_t)qe_accum_rows<R>(nb) * kMaxWindow * 2 * nb * sizeof(double2) +     // S | D
+         (size_t)kMaxWindow * kQeG * (size_t)(qe_accum_threads(n_en, nb) / nb) *
+             sizeof(double2);                                                       // coefficients
 }
 // Shared memory of qe_project_kernel.
-__host__ __device__ constexpr size_t qe_project_smem(int nb) {
-  return sizeof(double2) * (size_t)qe_tile_rows(nb) * kMaxProject * 2 * nb;
+template <typename R>
+__host__ __device__ constexpr size_t qe_project_smem(int n_en, int nb, int K) {
+  return (sizeof(R) == 4 ? (size_t)qe_tile_rows<R>(nb) * kMaxProject * 2 * nb * sizeof(double2)
+                         : 0) +                                                     // converted u
+         2 * (size_t)qe_tile_rows<R>(nb) * kMaxProject * 2 * nb * 2 * sizeof(R) +   // raw u
+         2 * (size_t)qe_tile_rows<R>(nb) * kQeG * (qe_project_threads(n_en, nb, K) / K) * 2 *
+             sizeof(R);                                                             // raw QE
 }
 
 // QE[r][i][b] (+)= sum_tau c[tau][i] * pos_tau[r][b] + conj(c[tau][i]) * neg_tau[r][b]
 // pos/neg columns of a window state: b and nb + b (ld = 2 nb).  init: start
 // from wf0[r][b] (tbpm.f90:600-603).
-// Grid: x strides over tiles of qe_tile_rows(nb) rows, y over chunks of
-// blockDim.x elements (i, b) of a row.  The block stages the coefficients of
-// its energies once and the window values of a row tile (converted to double
-// once, instead of once per energy) in shared memory; each thread then folds
-// the window into its element of every row of the tile, in the same order and
-// with the same arithmetic as one thread per element.
+// c p + conj(c) m = Re(c) (p + m) + i Im(c) (p - m): the sum S = p + m and the
+// difference D = p - m of a row are formed once, in double, per staged tile,
+// and every energy then needs 4 FMAs per window state instead of 8.
+// Block: qe_accum_threads(n_en, nb) threads; thread t owns the elements
+// ib_lo + t + g * blockDim.x (g < kQeG): state b = t % nb, kQeG energies, for
+// every row of a tile; a coefficient read from shared memory serves the rows
+// of the tile and an S / D value serves kQeG energies.  A thread's QE values
+// of a tile are loaded before the tile's window values are staged, so both
+// are in flight together.  (The window tile is staged with plain loads: a
+// second, asynchronously filled buffer would halve the resident blocks.)
+// Grid: x strides over row tiles, y over chunks of kQeG * blockDim.x elements.
 template <typename R>
-__global__ void __launch_bounds__(256) qe_accum_kernel(typename Cx<R>::t* qe, int64_t n_rows,
-                                                       int n_en, int nb, StatePtrs<R> win,
-                                                       int T, const double2* coef, int init,
-                                                       const typename Cx<R>::t* wf0) {
+__global__ void __launch_bounds__(256, TBPM_QE_MINB_A) qe_accum_kernel(
+    typename Cx<R>::t* qe, int64_t n_rows, int n_en, int nb, StatePtrs<R> win, int T,
+    const double2* coef, int init, const typename Cx<R>::t* wf0) {
+  using C = typename Cx<R>::t;
+  constexpr int RM = TBPM_QE_ROWS_A;
   extern __shared__ double2 qsm[];
   const int n_ib = n_en * nb;
   const int ld = 2 * nb;
-  const int RS = qe_tile_rows(nb);
-  const int ib0 = blockIdx.y * blockDim.x;
-  const int ib = ib0 + threadIdx.x;
-  const bool active = ib < n_ib;
-  const int i = (active ? ib : ib0) / nb;
-  const int b = active ? ib - i * nb : 0;
-  const int i0 = ib0 / nb;
-  const int ni = min(n_en, (ib0 + (int)blockDim.x - 1) / nb + 1) - i0;
-  double2* sc = qsm;                    // [kMaxWindow][ni]
-  double2* sw = qsm + kMaxWindow * ni;  // [RS][kMaxWindow][ld]
+  const int RS = qe_accum_rows<R>(nb);
+  const int NT = blockDim.x;  // a multiple of nb
+  const int EBE = kQeG * NT;  // elements of a row the block covers
+  const int ib_lo = blockIdx.y * EBE;
+  const int eb = min(EBE, n_ib - ib_lo);
+  const int t = threadIdx.x;
+  const int b = t % nb;
+  const int i_lo = ib_lo / nb;
+  const int ni = min(n_en - i_lo, EBE / nb);
+  bool act[kQeG];
+  int il[kQeG];  // energy of element g, relative to i_lo
+#pragma unroll
+  for (int g = 0; g < kQeG; ++g) {
+    act[g] = t + g * NT < eb;
+    il[g] = (t + g * NT) / nb;
+  }
+  const int TW = kMaxWindow * ld;                  // staged values of one row
+  double2* sd = qsm;                               // [RS][TW] S | D
+  double2* sc = qsm + RS * TW;                     // [kMaxWindow][ni]
   for (int q = threadIdx.x; q < T * ni; q += blockDim.x) {
     const int tau = q / ni;
     const int ii = q - tau * ni;
-    sc[tau * ni + ii] = coef[tau * n_en + i0 + ii];
+    sc[tau * ni + ii] = coef[tau * n_en + i_lo + ii];
   }
   for (int64_t rb = (int64_t)blockIdx.x * RS; rb < n_rows; rb += (int64_t)gridDim.x * RS) {
     const int nr = (int)min((int64_t)RS, n_rows - rb);
+    C q0[RM][kQeG];
+#pragma unroll
+    for (int rr = 0; rr < RM; ++rr)
+#pragma unroll
+      for (int g = 0; g < kQeG; ++g)
+        if (rr < nr && act[g])
+          q0[rr][g] = init ? wf0[(rb + rr) * nb + b] : qe[(rb + rr) * n_ib + ib_lo + t + g * NT];
     __syncthreads();  // the previous tile is consumed (and the coefficients staged)
 #pragma unroll
     for (int tau = 0; tau < kMaxWindow; ++tau) {
       if (tau < T) {
-        const typename Cx<R>::t* src = win.p[tau] + rb * ld;
-        for (int q = threadIdx.x; q < nr * ld; q += blockDim.x) {
-          const int rr = q / ld;
-          const typename Cx<R>::t v = ldg_c(src + q);
-          sw[(rr * kMaxWindow + tau) * ld + (q - rr * ld)] = make_double2((double)v.x, (double)v.y);
+        const C* src = win.p[tau] + rb * ld;
+        for (int q = threadIdx.x; q < nr * nb; q += blockDim.x) {
+          const int rr = q / nb;
+          const int bb = q - rr * nb;
+          const C p = ldg_c(src + rr * ld + bb);
+          const C m = ldg_c(src + rr * ld + nb + bb);
+          double2* o = sd + rr * TW + tau * ld;
+          o[bb] = make_double2((double)p.x + (double)m.x, (double)p.y + (double)m.y);
+          o[nb + bb] = make_double2((double)p.x - (double)m.x, (double)p.y - (double)m.y);
         }
       }
     }
     __syncthreads();
-    if (!active) continue;
-    for (int rr = 0; rr < nr; ++rr) {
-      const int64_t r = rb + rr;
-      const int64_t g = r * n_ib + ib;
-      double qr, qi;
-      if (init) {
-        const typename Cx<R>::t w = wf0[r * nb + b];
-        qr = (double)w.x;
-        qi = (double)w.y;
-      } else {
-        const typename Cx<R>::t q = qe[g];
-        qr = (double)q.x;
-        qi = (double)q.y;
-      }
-      const double2* wr = sw + rr * kMaxWindow * ld;
+    if (!act[0]) continue;
+    double qr[RM][kQeG], qi[RM][kQeG];
 #pragma unroll
-      for (int tau = 0; tau < kMaxWindow; ++tau) {
-        if (tau < T) {
-          const double2 c = sc[tau * ni + (i - i0)];
-          const double2 p = wr[tau * ld + b];
-          const double2 m = wr[tau * ld + nb + b];
-          const double pr = p.x, pi = p.y, mr = m.x, mi = m.y;
-          // c*p + conj(c)*m
-          qr += c.x * pr - c.y * pi + c.x * mr + c.y * mi;
-          qi += c.x * pi + c.y * pr + c.x * mi - c.y * mr;
+    for (int rr = 0; rr < RM; ++rr)
+#pragma unroll
+      for (int g = 0; g < kQeG; ++g) {
+        qr[rr][g] = (double)q0[rr][g].x;
+        qi[rr][g] = (double)q0[rr][g].y;
+      }
+#pragma unroll
+    for (int tau = 0; tau < kMaxWindow; ++tau) {
+      if (tau < T) {
+        double2 c[kQeG];
+#pragma unroll
+        for (int g = 0; g < kQeG; ++g) c[g] = act[g] ? sc[tau * ni + il[g]] : make_double2(0, 0);
+#pragma unroll
+        for (int rr = 0; rr < RM; ++rr) {
+          if (rr < nr) {
+            const double2 S = sd[rr * TW + tau * ld + b];
+            const double2 D = sd[rr * TW + tau * ld + nb + b];
+#pragma unroll
+            for (int g = 0; g < kQeG; ++g) {
+              qr[rr][g] += c[g].x * S.x - c[g].y * D.y;
+              qi[rr][g] += c[g].x * S.y + c[g].y * D.x;
+            }
+          }
         }
       }
-      typename Cx<R>::t o;
-      o.x = (R)qr;
-      o.y = (R)qi;
-      qe[g] = o;
     }
+#pragma unroll
+    for (int rr = 0; rr < RM; ++rr)
+#pragma unroll
+      for (int g = 0; g < kQeG; ++g)
+        if (rr < nr && act[g]) {
+          C o;
+          o.x = (R)qr[rr][g];
+          o.y = (R)qi[rr][g];
+          qe[(rb + rr) * n_ib + ib_lo + t + g * NT] = o;
+        }
   }
 }
 
-// Tall-skinny reductions over orbitals with one thread per (energy, state)
-// element: block partial sums of conj(u_tau[r][k*nb + b]) * QE[r][i][b] for
-// tau < T, k in {0, 1} (mode 0), or of conj(wf0[r][b]) * QE[r][i][b] (mode 1,
-// T = 1, k = 0).  partials[((tau*2 + k) * n_en*nb + ib) * 2 + {re,im}][block x].
-// Grid: x over row ranges of rows_per_tile, y over chunks of blockDim.x
-// elements.  The u values of a tile of rows are staged in shared memory as
-// double (converted once, not once per energy); each thread sums its rows in
-// order, with the accumulators in registers (compile-time indices only).
+// Tall-skinny reductions over orbitals: block partial sums of
+// conj(u_tau[r][k*nb + b]) * QE[r][i][b] for tau < T, k in {0, 1} (mode 0), or
+// of conj(wf0[r][b]) * QE[r][i][b] (mode 1, T = 1, k = 0).
+// partials[((tau*K + k) * n_en*nb + ib) * 2 + {re,im}][block x].
+// Block: qe_project_threads(n_en, nb, K) threads; thread t has k = t % K and
+// owns the elements ib_lo + t / K + g * (blockDim.x / K), g < kQeG (one state
+// b, kQeG energies); its T x kQeG accumulators stay in registers.
+// Grid: x over row ranges of rows_per_tile, y over chunks of elements.  Each
+// thread sums its rows in order.
 template <typename R>
-__global__ void __launch_bounds__(256) qe_project_kernel(const typename Cx<R>::t* qe,
-                                                         int64_t n_rows, int64_t rows_per_tile,
-                                                         int n_en, int nb, StatePtrs<R> u,
-                                                         int T, int mode,
-                                                         const typename Cx<R>::t* wf0,
-                                                         double* partials) {
+__global__ void __launch_bounds__(256, TBPM_QE_MINB_P) qe_project_kernel(
+    const typename Cx<R>::t* qe, int64_t n_rows, int64_t rows_per_tile, int n_en, int nb,
+    StatePtrs<R> u, int T, int mode, const typename Cx<R>::t* wf0, double* partials) {
+  using C = typename Cx<R>::t;
   extern __shared__ double2 qsm[];
   const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
   const int64_t r1 = min(r0 + rows_per_tile, n_rows);
   const int n_ib = n_en * nb;
   const int K = mode == 0 ? 2 : 1;
   const int ld = 2 * nb;
-  const int RS = qe_tile_rows(nb);
-  const int ib = blockIdx.y * blockDim.x + threadIdx.x;
-  const bool active = ib < n_ib;
-  const int b = active ? ib % nb : 0;
-  double ar[2 * kMaxProject], ai[2 * kMaxProject];
+  const int RS = qe_tile_rows<R>(nb);
+  const int NE = blockDim.x / K;  // threads per k, a multiple of nb
+  const int EBE = kQeG * NE;      // elements of a row the block covers
+  const int ib_lo = blockIdx.y * EBE;
+  const int eb = min(EBE, n_ib - ib_lo);
+  const int k = threadIdx.x % K;
+  const int e = threadIdx.x / K;
+  const int b = e % nb;
+  bool act[kQeG];
 #pragma unroll
-  for (int q = 0; q < 2 * kMaxProject; ++q) ar[q] = ai[q] = 0.0;
-  for (int64_t rb = r0; rb < r1; rb += RS) {
+  for (int g = 0; g < kQeG; ++g) act[g] = e + g * NE < eb;
+  const int UW = kMaxProject * ld;  // staged values of one row
+  constexpr bool conv = sizeof(R) == 4;
+  double2* dbl = qsm;                                               // [RS][UW] (FP32 only)
+  C* raw_u = reinterpret_cast<C*>(qsm + (conv ? RS * UW : 0));      // [2][RS][UW]
+  C* raw_q = raw_u + 2 * RS * UW;                                   // [2][RS][EBE]
+  auto issue = [&](int64_t rb, int buf) {
     const int nr = (int)min((int64_t)RS, r1 - rb);
-    __syncthreads();  // the previous tile is consumed
-    if (mode == 1) {
-      for (int q = threadIdx.x; q < nr * nb; q += blockDim.x) {
-        const typename Cx<R>::t v = ldg_c(wf0 + rb * nb + q);
-        qsm[q] = make_double2((double)v.x, (double)v.y);
-      }
-    } else {
+    C* du = raw_u + buf * RS * UW;
+    if (mode == 0) {
 #pragma unroll
       for (int tau = 0; tau < kMaxProject; ++tau) {
         if (tau < T) {
-          const typename Cx<R>::t* src = u.p[tau] + rb * ld;
+          const C* src = u.p[tau] + rb * ld;
           for (int q = threadIdx.x; q < nr * ld; q += blockDim.x) {
             const int rr = q / ld;
-            const typename Cx<R>::t v = ldg_c(src + q);
-            qsm[(rr * kMaxProject + tau) * ld + (q - rr * ld)] =
-                make_double2((double)v.x, (double)v.y);
+            qe_cp_async(du + rr * UW + tau * ld + (q - rr * ld), src + q);
           }
         }
       }
+    } else {
+      for (int q = threadIdx.x; q < nr * nb; q += blockDim.x) {
+        const int rr = q / nb;
+        qe_cp_async(du + rr * UW + (q - rr * nb), wf0 + rb * nb + q);
+      }
     }
-    __syncthreads();
-    if (!active) continue;
+    C* dq = raw_q + buf * RS * EBE;
+    for (int q = threadIdx.x; q < nr * eb; q += blockDim.x) {
+      const int rr = q / eb;
+      const int ee = q - rr * eb;
+      qe_cp_async(dq + rr * EBE + ee, qe + (rb + rr) * n_ib + ib_lo + ee);
+    }
+  };
+  double ar[kMaxProject][kQeG], ai[kMaxProject][kQeG];
+#pragma unroll
+  for (int q = 0; q < kMaxProject; ++q)
+#pragma unroll
+    for (int g = 0; g < kQeG; ++g) ar[q][g] = ai[q][g] = 0.0;
+  if (r0 < r1) issue(r0, 0);
+  qe_cp_commit();
+  int j = 0;
+  for (int64_t rb = r0; rb < r1; rb += RS, ++j) {
+    const int nr = (int)min((int64_t)RS, r1 - rb);
+    qe_cp_wait_all();
+    __syncthreads();  // tile j is in shared memory; tile j-1 is consumed
+    if (rb + RS < r1) issue(rb + RS, (j + 1) & 1);
+    qe_cp_commit();
+    const C* tu = raw_u + (j & 1) * RS * UW;
+    const C* tq = raw_q + (j & 1) * RS * EBE;
+    if constexpr (conv) {
+      const int per_row = mode == 0 ? T * ld : nb;
+      for (int q = threadIdx.x; q < nr * per_row; q += blockDim.x) {
+        const int rr = q / per_row;
+        const int w = q - rr * per_row;
+        const C v = tu[rr * UW + w];
+        dbl[rr * UW + w] = make_double2((double)v.x, (double)v.y);
+      }
+      __syncthreads();
+    }
+    if (!act[0]) continue;
     for (int rr = 0; rr < nr; ++rr) {
-      const typename Cx<R>::t qv = qe[(rb + rr) * n_ib + ib];
-      const double qr = (double)qv.x, qi = (double)qv.y;
+      double qr[kQeG], qi[kQeG];
+#pragma unroll
+      for (int g = 0; g < kQeG; ++g) {
+        const C qv = act[g] ? tq[rr * EBE + e + g * NE] : C{};
+        qr[g] = (double)qv.x;
+        qi[g] = (double)qv.y;
+      }
       if (mode == 1) {
-        const double2 w = qsm[rr * nb + b];
-        ar[0] += w.x * qr + w.y * qi;
-        ai[0] += w.x * qi - w.y * qr;
+        double2 w;
+        if constexpr (conv)
+          w = dbl[rr * UW + b];
+        else
+          w = make_double2((double)tu[rr * UW + b].x, (double)tu[rr * UW + b].y);
+#pragma unroll
+        for (int g = 0; g < kQeG; ++g) {
+          ar[0][g] += w.x * qr[g] + w.y * qi[g];
+          ai[0][g] += w.x * qi[g] - w.y * qr[g];
+        }
       } else {
-        const double2* ur = qsm + rr * kMaxProject * ld;
 #pragma unroll
         for (int tau = 0; tau < kMaxProject; ++tau) {
           if (tau < T) {
+            const int o = rr * UW + tau * ld + k * nb + b;
+            double2 w;
+            if constexpr (conv)
+              w = dbl[o];
+            else
+              w = make_double2((double)tu[o].x, (double)tu[o].y);
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-              const double2 w = ur[tau * ld + k * nb + b];
-              ar[tau * 2 + k] += w.x * qr + w.y * qi;
-              ai[tau * 2 + k] += w.x * qi - w.y * qr;
+            for (int g = 0; g < kQeG; ++g) {
+              ar[tau][g] += w.x * qr[g] + w.y * qi[g];
+              ai[tau][g] += w.x * qi[g] - w.y * qr[g];
             }
           }
         }
       }
     }
   }
-  if (!active) return;
 #pragma unroll
-  for (int q = 0; q < 2 * kMaxProject; ++q) {
-    if (q < T * K) {
-      const int64_t o = (int64_t)q * n_ib + ib;
-      partials[(o * 2 + 0) * gridDim.x + blockIdx.x] = ar[q];
-      partials[(o * 2 + 1) * gridDim.x + blockIdx.x] = ai[q];
+  for (int g = 0; g < kQeG; ++g) {
+    if (!act[g]) continue;
+    const int ib = ib_lo + e + g * NE;
+#pragma unroll
+    for (int tau = 0; tau < kMaxProject; ++tau) {
+      if (tau < (mode == 0 ? T : 1)) {
+        const int64_t o = (int64_t)(tau * K + k) * n_ib + ib;
+        partials[(o * 2 + 0) * gridDim.x + blockIdx.x] = ar[tau][g];
+        partials[(o * 2 + 1) * gridDim.x + blockIdx.x] = ai[tau][g];
+      }
     }
   }
 }

@@ -914,15 +914,23 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
 // One batch of nb states of tbpm_dccond (tbpm.f90:586-698), or, with qe_acc
 // set, of tbpm_eigenstates (tbpm.f90:753-813): phase 1 only, then every
 // quasi-eigenstate is normalised and acc[r][i] += |QE_i(r)|^2 / n_avg.
-// qe_accum_kernel may need more than the default 48 KB of dynamic shared
-// memory (many energies per block when nb is small).
-template <typename R>
-void qe_smem_attr(size_t bytes) {
-  static size_t granted = 48 * 1024;
+// The QE kernels may need more than the default 48 KB of dynamic shared
+// memory (double-buffered row tiles).
+template <class K>
+void qe_smem_attr(K kernel, size_t bytes, size_t& granted) {
   if (bytes <= granted) return;
-  TBPM_CK(cudaFuncSetAttribute(qe_accum_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)bytes));
+  TBPM_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   granted = bytes;
+}
+template <typename R>
+void qe_accum_attr(size_t bytes) {
+  static size_t granted = 48 * 1024;
+  qe_smem_attr(qe_accum_kernel<R>, bytes, granted);
+}
+template <typename R>
+void qe_project_attr(size_t bytes) {
+  static size_t granted = 48 * 1024;
+  qe_smem_attr(qe_project_kernel<R>, bytes, granted);
 }
 
 template <typename R, int V>
@@ -1002,12 +1010,12 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       StatePtrs<R> win{};
       for (int tau = 0; tau < len; ++tau) win.p[tau] = reinterpret_cast<const C*>(slot(tau));
       const int64_t total = n * n_en * nb;
-      const int qthreads = std::min(256, ((n_en * nb + 31) / 32) * 32);
-      const int n_chunks = (n_en * nb + qthreads - 1) / qthreads;
-      const int64_t tiles = (n + qe_tile_rows(nb) - 1) / qe_tile_rows(nb);
-      const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)kSMs * 8), (unsigned)n_chunks);
-      const size_t qsmem = qe_accum_smem(n_en, nb, qthreads);
-      qe_smem_attr<R>(qsmem);
+      const int qthreads = qe_accum_threads(n_en, nb);
+      const int n_chunks = (n_en * nb + kQeG * qthreads - 1) / (kQeG * qthreads);
+      const int64_t tiles = (n + qe_accum_rows<R>(nb) - 1) / qe_accum_rows<R>(nb);
+      const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)kSMs * 16), (unsigned)n_chunks);
+      const size_t qsmem = qe_accum_smem<R>(n_en, nb);
+      qe_accum_attr<R>(qsmem);
       qe_accum_kernel<R><<<grid, qthreads, qsmem, c->stream>>>(qe, n, n_en, nb, win, len,
                                                         c->coef.as<double2>(),
                                                         first_window ? 1 : 0,
@@ -1067,14 +1075,21 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   const int n_ib = n_en * nb;
   int64_t rows_per_tile = std::max<int64_t>(64, n / ((int64_t)kSMs * 8));
   const int pgrid = (int)((n + rows_per_tile - 1) / rows_per_tile);
-  const int pthreads = std::min(256, ((n_ib + 31) / 32) * 32);
-  const dim3 pgrid2((unsigned)pgrid, (unsigned)((n_ib + pthreads - 1) / pthreads));
-  const size_t psmem = qe_project_smem(nb);
+  // mode 1 (one projection): one thread per kQeG elements; mode 0: a pair
+  const int pthreads1 = qe_project_threads(n_en, nb, 1);
+  const dim3 pgrid1((unsigned)pgrid,
+                    (unsigned)((n_ib + kQeG * pthreads1 - 1) / (kQeG * pthreads1)));
+  const int pthreads = qe_project_threads(n_en, nb, 2);
+  const dim3 pgrid2((unsigned)pgrid,
+                    (unsigned)((n_ib + kQeG * (pthreads / 2) - 1) / (kQeG * (pthreads / 2))));
+  const size_t psmem1 = qe_project_smem<R>(n_en, nb, 1);
+  const size_t psmem = qe_project_smem<R>(n_en, nb, 2);
+  qe_project_attr<R>(std::max(psmem1, psmem));
   // |<wf0|QE_i>| per (energy, state)
   ensure_partials(c, (size_t)2 * n_ib * pgrid);
   c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
-  qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
-                                                               StatePtrs<R>{}, 1, 1,
+  qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
+                                                                StatePtrs<R>{}, 1, 1,
                                                           reinterpret_cast<const C*>(W),
                                                           c->partials.as<double>());
   TBPM_CK(cudaGetLastError());
