@@ -225,7 +225,7 @@ def run_c5(steps: int = 2048, n_states: int = 8, nx: int = 4096, precision: str 
     return {"workload": f"c5 graphene {nx}x{nx}, B={b_field:.2f} T (flux h/e per 1024 "
                         f"hexagons), W=1 eV, {n_states} states, corr_dc {precision}",
             "builder": builder, "n_orbitals": int(n), "steps": steps,
-            "n_energies": int(energies.size),
+            "n_energies": int(energies.size), "energy_limits_eV": list(energy_limits),
             "build_seconds": t_build, "seconds": sec,
             "orbital_steps_per_s": n * n_states * steps / sec,
             "sigma_dc_xx_at_E0": float(dc[0, i0]), "sigma_dc_yy_at_E0": float(dc[1, i0]),
@@ -531,6 +531,9 @@ def main(argv=None) -> None:
                     help="c5: assemble the Hamiltonian on the GPU or on the host")
     ap.add_argument("--nx", type=int, default=None,
                     help="c5: cells per side (default 4096)")
+    ap.add_argument("--energy-limits", type=float, nargs=2, default=None,
+                    help="c5: energy window of the DC conductivity in eV (default -0.5 0.5); "
+                         "the quasi-eigenstate block holds N x energies x states values")
     args = ap.parse_args(argv)
     for w in args.workloads:
         kw = {}
@@ -543,6 +546,8 @@ def main(argv=None) -> None:
             kw["builder"] = args.builder
             if args.nx:
                 kw["nx"] = args.nx
+            if args.energy_limits:
+                kw["energy_limits"] = tuple(args.energy_limits)
         r = RUNNERS[w](**kw)
         line = json.dumps(r)
         print(line, flush=True)
