@@ -201,7 +201,9 @@ def run_gpu(args):
     for prec_name, prec in (("fp64", nat.PREC_FP64), ("fp32", nat.PREC_FP32)):
         if prec_name == "fp32" and args.skip_fp32:
             continue
-        ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=16)
+        ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=16,
+                        vector_width=args.vector_width if prec_name == "fp64" else 0,
+                        threads_per_block=args.threads if prec_name == "fp64" else 0)
         ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, None, None,
                  sample.rescale)
         total = args.steps + args.warmup
@@ -260,7 +262,8 @@ def run_gpu(args):
             f"{results[prec_name]['achieved_gbs']:.0f} GB/s, launches {launches}")
 
     # ---- e2e through the public API (FP64, host buffers) -----------------
-    f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True)
+    f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True,
+                     vector_width=args.vector_width, threads_per_block=args.threads)
     from tbplas_b200.parallel import MPIEnv
     env = MPIEnv(enable_mpi=distributed)
     e2e_steps = args.steps
@@ -321,7 +324,7 @@ def run_gpu(args):
                 "traffic_note": "bytes per step: ncu DRAM bytes / algorithmic bytes = 0.982 on "
                                 "the 1024x1024 case, scaled by rows to this workload",
                 "alg_bytes_per_step": r64["alg_bytes_per_step"],
-                "kernel": "cheb_term_kernel<double,1> (+ finalize_kernel, <1% of step)",
+                "kernel": "cheb_term_kernel<double,2> (+ finalize_kernel, <1% of step)",
             },
             "e2e": e2e,
             "gpu_launches": int(r64["launches"]),
@@ -424,6 +427,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--vector-width", type=int, default=0, choices=[0, 1, 2],
+                    help="FP64 complex values per thread: 0 library default (two, 256-bit "
+                         "accesses), 1 one (128-bit accesses), 2 two")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="FP64 threads per block of the term kernel (0: library default)")
     ap.add_argument("--nx", type=int, default=2048,
                     help="cells along a1 (smaller values only for profiling captures)")
     ap.add_argument("--ny", type=int, default=2048)

@@ -54,6 +54,15 @@ __device__ __forceinline__ Pack<float, 1> ldg_pack(const Pack<float, 1>* p) {
   return r;
 }
 
+// Two complex128 values per thread: one 256-bit access (ld/st .v4.f64, sm_100).
+__device__ __forceinline__ Pack<double, 2> ldg_pack(const Pack<double, 2>* p) {
+  Pack<double, 2> r;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3])
+      : "l"(p));
+  return r;
+}
+
 // Streaming (evict-first) access for vectors read or written once per kernel,
 // so they do not push the gathered vector out of L2.
 __device__ __forceinline__ Pack<double, 1> ldcs_pack(const Pack<double, 1>* p) {
@@ -78,6 +87,19 @@ __device__ __forceinline__ Pack<float, 1> ldcs_pack(const Pack<float, 1>* p) {
   r.v[0] = d.x;
   r.v[1] = d.y;
   return r;
+}
+__device__ __forceinline__ Pack<double, 2> ldcs_pack(const Pack<double, 2>* p) {
+  Pack<double, 2> r;
+  asm volatile("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ void stcs_pack(Pack<double, 2>* p, const Pack<double, 2>& v) {
+  asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.v[0]), "d"(v.v[1]),
+               "d"(v.v[2]), "d"(v.v[3])
+               : "memory");
 }
 __device__ __forceinline__ void stcs_pack(Pack<double, 1>* p, const Pack<double, 1>& v) {
   __stcs(reinterpret_cast<double2*>(p), make_double2(v.v[0], v.v[1]));

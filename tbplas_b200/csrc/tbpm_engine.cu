@@ -105,7 +105,9 @@ struct Prec {
 
 template <class F>
 void dispatch(int prec, int V, F&& f) {
-  if (prec == TBPM_PREC_FP64)
+  if (prec == TBPM_PREC_FP64 && V == 2)
+    f(Prec<double, 2>{});
+  else if (prec == TBPM_PREC_FP64)
     f(Prec<double, 1>{});
   else if (V == 2)
     f(Prec<float, 2>{});
@@ -371,6 +373,13 @@ void enqueue_corr(tbpm_ctx* c, const Pack<R, V>* x, const Pack<R, V>* ref, int l
 // columns starting at column 0).  keys[col] = iseed * 49741.
 template <typename R, int V>
 void gen_states(tbpm_ctx* c, const StateKeys& keys, int ld, int kind, Pack<R, V>* dst) {
+  if constexpr (sizeof(R) == 8 && V == 2) {
+    // Same memory layout; generating with one value per thread keeps the
+    // normalisation sums grouped as for every other FP64 caller (e.g.
+    // tbpm_random_states), so the states do not depend on the vector width.
+    gen_states<R, 1>(c, keys, ld, kind, reinterpret_cast<Pack<R, 1>*>(dst));
+    return;
+  }
   const int tpr = ld / V;
   const Tile t = pick_tile(c, c->ham.n, tpr, gen_state_kernel<R, V>, V * sizeof(double));
   ensure_partials(c, (size_t)ld * t.grid);
@@ -437,8 +446,10 @@ StateKeys make_keys(int seed, int first_sample, int n_states, int rank, int n_ra
 }
 
 int pick_V(int prec, int ld, int group, int requested = 0) {
-  if (prec == TBPM_PREC_FP64) return 1;
   const bool can2 = ld % 2 == 0 && group % 2 == 0;
+  // FP64: two complex128 per thread (256-bit accesses) unless one is requested
+  // (measured on B200, 2048^2 graphene, 16 states: 33.7 vs 37.6 ms per step)
+  if (prec == TBPM_PREC_FP64) return requested != 1 && can2 ? 2 : 1;
   if (requested == 1) return 1;
   return can2 ? 2 : 1;
 }
@@ -915,22 +926,20 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
 // set, of tbpm_eigenstates (tbpm.f90:753-813): phase 1 only, then every
 // quasi-eigenstate is normalised and acc[r][i] += |QE_i(r)|^2 / n_avg.
 // The QE kernels may need more than the default 48 KB of dynamic shared
-// memory (double-buffered row tiles).
+// memory (row tiles).  The attribute belongs to the current device, so it is
+// set before every launch that needs it (a host-side call, once per window).
 template <class K>
-void qe_smem_attr(K kernel, size_t bytes, size_t& granted) {
-  if (bytes <= granted) return;
+void qe_smem_attr(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
   TBPM_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  granted = bytes;
 }
 template <typename R>
 void qe_accum_attr(size_t bytes) {
-  static size_t granted = 48 * 1024;
-  qe_smem_attr(qe_accum_kernel<R>, bytes, granted);
+  qe_smem_attr(qe_accum_kernel<R>, bytes);
 }
 template <typename R>
 void qe_project_attr(size_t bytes) {
-  static size_t granted = 48 * 1024;
-  qe_smem_attr(qe_project_kernel<R>, bytes, granted);
+  qe_smem_attr(qe_project_kernel<R>, bytes);
 }
 
 template <typename R, int V>

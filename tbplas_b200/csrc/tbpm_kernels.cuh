@@ -70,10 +70,18 @@ struct TermArgs {
 #define TBPM_MINB_FLUSH 4
 #endif
 
-template <typename R, int MODE>
+// two complex128 values per thread (V = 2) hold twice the data in registers
+#ifndef TBPM_MINB_F64_V2
+#define TBPM_MINB_F64_V2 2
+#endif
+
+template <typename R, int MODE, int V = 1>
 struct TermBounds {
   static constexpr int min_blocks =
-      MODE == 0 ? (sizeof(R) == 8 ? TBPM_MINB_PLAIN_F64 : TBPM_MINB_PLAIN_F32) : TBPM_MINB_FLUSH;
+      sizeof(R) == 8 && V == 2
+          ? TBPM_MINB_F64_V2
+          : (MODE == 0 ? (sizeof(R) == 8 ? TBPM_MINB_PLAIN_F64 : TBPM_MINB_PLAIN_F32)
+                       : TBPM_MINB_FLUSH);
 };
 // independent gathers issued per batch
 #ifndef TBPM_BW
@@ -101,7 +109,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes, const 
 }
 
 template <typename R, int V, int MODE>
-__global__ void __launch_bounds__(256, (TermBounds<R, MODE>::min_blocks))
+__global__ void __launch_bounds__(256, (TermBounds<R, MODE, V>::min_blocks))
     cheb_term_kernel(const TermArgs<R, V> a) {
   extern __shared__ double smem[];
   constexpr int BW = TBPM_BW;

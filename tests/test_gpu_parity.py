@@ -289,3 +289,48 @@ def test_solver_drop_in(tmp_path, graphene_small):
     analyzer = tb.Analyzer(graphene_small, config, dimension=2)
     energies, dos = analyzer.calc_dos(corr)
     assert energies.shape == (64,) and abs(np.sum(dos) * (energies[1] - energies[0]) - 1) < 1e-12
+
+
+@pytest.mark.parametrize("width", [1, 2])
+@pytest.mark.parametrize("driver", ["dos", "ac", "dc", "psi_t"])
+def test_fp64_values_per_thread_match_oracle(graphene_small, dos_bes, ac_bes, driver, width):
+    """FP64 with one complex128 per thread (128-bit accesses) and with two
+    (256-bit loads and stores, the default for even block widths): results must
+    not depend on it."""
+    f2py.set_backend(vector_width=width)
+    try:
+        if driver == "dos":
+            ip, ix, hv = _csr(graphene_small)
+            wf0 = unit_states(6, ip.size - 1, seed=12)
+            got = f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0, 30, 128, 1e-9)
+            ref = oracle.tbpm_dos(dos_bes, ip, ix, hv, 30, wf0=wf0)
+        elif driver == "ac":
+            s = tb.make_graphene_sample(8, 6, disorder=0.6, rescale=9.0, seed=3)
+            ip, ix, hv, dx, dy = _dxy(s)
+            wf0 = unit_states(2, ip.size - 1, seed=21)
+            beta = 9.0 / (tb.KB * 300)
+            got = f2py.tbpm_accond_states(ac_bes, beta, 0.0, ip, ix, hv, s.rescale, dx, dy, wf0,
+                                          16, 2**15, 1e-12, 128, 1e-9)
+            ref = oracle.tbpm_accond(ac_bes, beta, 0.0, ip, ix, hv, s.rescale, dx, dy, 16,
+                                     wf0=wf0)
+        elif driver == "dc":
+            s = tb.make_graphene_sample(8, 6, disorder=0.8, rescale=9.0, seed=9)
+            ip, ix, hv, dx, dy = _dxy(s)
+            wf0 = unit_states(2, ip.size - 1, seed=31)
+            energies, qe = _dc_energies(s, 20, limits=(-2.0, 2.0))
+            t_step = 2 * math.pi / s.energy_range
+            got = f2py.tbpm_dccond_states(dos_bes, ip, ix, hv, s.rescale, dx, dy, wf0, 20,
+                                          t_step, energies, qe, 128, 1e-9)
+            ref = oracle.tbpm_dccond(dos_bes, ip, ix, hv, s.rescale, dx, dy, 20, t_step,
+                                     energies, qe, wf0=wf0)
+            assert rel_err(got[0], ref[0]) < FP64_TOL
+            got, ref = got[1], ref[1]
+        else:
+            ip, ix, hv = _csr(graphene_small)
+            psi0 = unit_states(1, ip.size - 1, seed=41)[0]
+            got = f2py.tbpm_psi_t(dos_bes, ip, ix, hv, psi0, np.array([0, 3, 11]), 11, 128,
+                                  1e-9)
+            ref = oracle.tbpm_psi_t(dos_bes, ip, ix, hv, psi0, np.array([0, 3, 11]), 11)
+        assert rel_err(got, ref) < FP64_TOL
+    finally:
+        f2py.set_backend(vector_width=0)
