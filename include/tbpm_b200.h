@@ -64,7 +64,8 @@ typedef struct tbpm_options {
   double fp32_chk_thr;   /* lower bound of the norm-check threshold in FP32
                             mode (default 1e-4); FP64 uses wfn_chk_thr as is */
   int vector_width;      /* complex values per thread and load.  FP32: 0 = automatic
-                            (2 when the block width allows), 1, 2.  FP64: 0 = automatic
+                            (4, with 256-bit accesses, when the block width is a
+                            multiple of 4, else 2 when even), 1, 2.  FP64: 0 = automatic
                             (two complex128 per thread with 256-bit accesses when the
                             block width allows), 1 = one (128-bit accesses), 2 */
 } tbpm_options;

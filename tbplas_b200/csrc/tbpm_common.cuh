@@ -63,6 +63,16 @@ __device__ __forceinline__ Pack<double, 2> ldg_pack(const Pack<double, 2>* p) {
   return r;
 }
 
+// Four complex64 values per thread: one 256-bit access (ld/st .v8.f32, sm_100).
+__device__ __forceinline__ Pack<float, 4> ldg_pack(const Pack<float, 4>* p) {
+  Pack<float, 4> r;
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]),
+        "=f"(r.v[6]), "=f"(r.v[7])
+      : "l"(p));
+  return r;
+}
+
 // Streaming (evict-first) access for vectors read or written once per kernel,
 // so they do not push the gathered vector out of L2.
 __device__ __forceinline__ Pack<double, 1> ldcs_pack(const Pack<double, 1>* p) {
@@ -99,6 +109,21 @@ __device__ __forceinline__ Pack<double, 2> ldcs_pack(const Pack<double, 2>* p) {
 __device__ __forceinline__ void stcs_pack(Pack<double, 2>* p, const Pack<double, 2>& v) {
   asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.v[0]), "d"(v.v[1]),
                "d"(v.v[2]), "d"(v.v[3])
+               : "memory");
+}
+__device__ __forceinline__ Pack<float, 4> ldcs_pack(const Pack<float, 4>* p) {
+  Pack<float, 4> r;
+  asm volatile("ld.global.cs.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]),
+                 "=f"(r.v[5]), "=f"(r.v[6]), "=f"(r.v[7])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ void stcs_pack(Pack<float, 4>* p, const Pack<float, 4>& v) {
+  asm volatile("st.global.cs.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p),
+               "f"(v.v[0]), "f"(v.v[1]), "f"(v.v[2]), "f"(v.v[3]), "f"(v.v[4]), "f"(v.v[5]),
+               "f"(v.v[6]), "f"(v.v[7])
                : "memory");
 }
 __device__ __forceinline__ void stcs_pack(Pack<double, 1>* p, const Pack<double, 1>& v) {

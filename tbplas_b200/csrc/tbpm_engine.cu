@@ -109,6 +109,8 @@ void dispatch(int prec, int V, F&& f) {
     f(Prec<double, 2>{});
   else if (prec == TBPM_PREC_FP64)
     f(Prec<double, 1>{});
+  else if (V == 4)
+    f(Prec<float, 4>{});
   else if (V == 2)
     f(Prec<float, 2>{});
   else
@@ -247,12 +249,15 @@ struct TermTiles {
   Tile t[3];
 };
 
+#ifndef TBPM_F32V4_THREADS
+#define TBPM_F32V4_THREADS 128
+#endif
 template <typename R, int V>
 TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr) {
   TermTiles tt;
   // measured on B200 (2048^2 graphene, 16 states): 128-thread blocks for FP64,
   // 256 for FP32
-  const int th = sizeof(R) == 8 ? 128 : 256;
+  const int th = sizeof(R) == 8 ? 128 : (V == 4 ? TBPM_F32V4_THREADS : 256);
   tt.t[0] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 0>, 0, th);
   tt.t[1] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 1>, 0, th);
   tt.t[2] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 2>, V * 3 * sizeof(double), th);
@@ -445,13 +450,19 @@ StateKeys make_keys(int seed, int first_sample, int n_states, int rank, int n_ra
   return k;
 }
 
+#ifndef TBPM_FP32_V4
+#define TBPM_FP32_V4 1
+#endif
 int pick_V(int prec, int ld, int group, int requested = 0) {
   const bool can2 = ld % 2 == 0 && group % 2 == 0;
   // FP64: two complex128 per thread (256-bit accesses) unless one is requested
   // (measured on B200, 2048^2 graphene, 16 states: 33.7 vs 37.6 ms per step)
   if (prec == TBPM_PREC_FP64) return requested != 1 && can2 ? 2 : 1;
   if (requested == 1) return 1;
-  return can2 ? 2 : 1;
+  // FP32: four complex64 per thread (256-bit accesses) when the widths allow
+  const bool can4 = ld % 4 == 0 && group % 4 == 0;
+  if (requested == 2 || TBPM_FP32_V4 == 0) return can2 ? 2 : 1;
+  return can4 ? 4 : (can2 ? 2 : 1);
 }
 
 void require_ham(const tbpm_ctx* c, bool need_dxy) {

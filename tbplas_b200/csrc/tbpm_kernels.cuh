@@ -70,7 +70,8 @@ struct TermArgs {
 #define TBPM_MINB_FLUSH 4
 #endif
 
-// two complex128 values per thread (V = 2) hold twice the data in registers
+// 32 bytes of state per thread (two complex128 or four complex64) hold twice
+// the data in registers
 #ifndef TBPM_MINB_F64_V2
 #define TBPM_MINB_F64_V2 2
 #endif
@@ -78,7 +79,7 @@ struct TermArgs {
 template <typename R, int MODE, int V = 1>
 struct TermBounds {
   static constexpr int min_blocks =
-      sizeof(R) == 8 && V == 2
+      sizeof(R) * V == 16
           ? TBPM_MINB_F64_V2
           : (MODE == 0 ? (sizeof(R) == 8 ? TBPM_MINB_PLAIN_F64 : TBPM_MINB_PLAIN_F32)
                        : TBPM_MINB_FLUSH);

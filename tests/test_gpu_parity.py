@@ -334,3 +334,37 @@ def test_fp64_values_per_thread_match_oracle(graphene_small, dos_bes, ac_bes, dr
         assert rel_err(got, ref) < FP64_TOL
     finally:
         f2py.set_backend(vector_width=0)
+
+
+@pytest.mark.parametrize("width", [0, 1, 2])
+@pytest.mark.parametrize("driver", ["dos", "ac", "dc"])
+def test_fp32_values_per_thread_within_bounds(dos_bes, ac_bes, driver, width):
+    """FP32 states with four complex64 per thread (256-bit accesses, the default
+    when the block width is a multiple of 4), two, and one: each within the FP32
+    bound of the oracle (2e-5 relative over these short runs), whatever the width."""
+    s = tb.make_graphene_sample(8, 6, disorder=0.6, rescale=9.0, seed=3)
+    ip, ix, hv, dx, dy = _dxy(s)
+    n = ip.size - 1
+    wf0 = unit_states(4, n, seed=27)
+    f2py.set_backend(precision="fp32", vector_width=width)
+    try:
+        if driver == "dos":
+            h = s.build_ham_csr()
+            got = f2py.tbpm_dos_states(dos_bes, h.indptr, h.indices, h.data, wf0, 24, 128, 1e-9)
+            ref = oracle.tbpm_dos(dos_bes, h.indptr, h.indices, h.data, 24, wf0=wf0)
+        elif driver == "ac":
+            beta = 9.0 / (tb.KB * 300)
+            got = f2py.tbpm_accond_states(ac_bes, beta, 0.0, ip, ix, hv, s.rescale, dx, dy, wf0,
+                                          12, 2**15, 1e-12, 128, 1e-9)
+            ref = oracle.tbpm_accond(ac_bes, beta, 0.0, ip, ix, hv, s.rescale, dx, dy, 12,
+                                     wf0=wf0)
+        else:
+            energies, qe = _dc_energies(s, 16, limits=(-2.0, 2.0))
+            t_step = 2 * math.pi / s.energy_range
+            got = f2py.tbpm_dccond_states(dos_bes, ip, ix, hv, s.rescale, dx, dy, wf0, 16,
+                                          t_step, energies, qe, 128, 1e-9)[1]
+            ref = oracle.tbpm_dccond(dos_bes, ip, ix, hv, s.rescale, dx, dy, 16, t_step,
+                                     energies, qe, wf0=wf0)[1]
+        assert rel_err(got, ref) < 2e-5
+    finally:
+        f2py.set_backend(precision="fp64", vector_width=0)
