@@ -50,7 +50,14 @@ def tune_dos(indptr, indices, hop, n_states: int, precision: str = "fp64",
         bessel = np.array([spec.jv(i, math.pi) for i in range(20)])
     bes = nat.as_c(bessel, np.float64)
     prec = nat.PREC_FP64 if precision == "fp64" else nat.PREC_FP32
-    widths = (1, 2) if (precision == "fp32" and n_states % 2 == 0) else (0,)
+    # vector widths: 0 = the library's choice (32-byte accesses when the block
+    # width allows: four complex64 / two complex128 per thread), 1, 2 forced
+    if n_states % 2:
+        widths = (0,)
+    elif precision == "fp32":
+        widths = (0, 1, 2)
+    else:
+        widths = (0, 1)
     timings = []
     saved = ctx.options
     try:

@@ -35,7 +35,7 @@ _backend = {
     "steps_per_graph": 16,
     "use_graphs": True,
     "fp32_chk_thr": 1.0e-4,
-    "vector_width": 0,       # FP32 complex values per thread: 0 auto, 1, 2
+    "vector_width": 0,       # complex values per thread: 0 auto (32-byte accesses), 1, 2
     "verbose": False,
 }
 
