@@ -3,9 +3,9 @@
 A short propagation gives C(t) for t = 0..n_in; the network predicts
 C(n_in+1 .. n_in+n_out) (real and imaginary parts), so that the DOS can be
 evaluated at the resolution of the full length without propagating it.  The
-full-length plain propagation remains the fallback and the judge: `evaluate`
-compares the DOS of (short propagation + predicted tail) with the DOS of the
-full propagation.
+full-length plain propagation remains the fallback and the yardstick:
+`evaluate` compares the DOS of (short propagation + predicted tail) with the
+DOS of the full propagation.
 
 Network (all dense/convolution products are the BF16 tensor-core GEMM of
 libtbpm_b200 with FP32 accumulation; activations channel-last):
