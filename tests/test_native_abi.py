@@ -124,3 +124,18 @@ def test_checkpoint_fingerprint_tracks_every_input(tmp_path):
     assert ck._load(path, variants[0]) is None
     (tmp_path / "bad.npz").write_bytes(b"not a zip")
     assert ck._load(str(tmp_path / "bad.npz"), base) is None
+
+
+def test_header_is_plain_c():
+    """include/tbpm_b200.h is the drop-in boundary for C FFIs (cgo, ctypes,
+    JNI stubs): it must compile as C99 on its own, with no C++ types."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    hdr = os.path.join(root, "include", "tbpm_b200.h")
+    r = subprocess.run([cc, "-x", "c", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", hdr],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
