@@ -139,3 +139,47 @@ def test_header_is_plain_c():
     r = subprocess.run([cc, "-x", "c", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", hdr],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_c_program_links_and_calls_host_entry_points(tmp_path):
+    """A plain C caller (as a cgo or JNI stub would be) links against
+    libtbpm_b200.so and calls the host-only entry points; its Fermi
+    coefficients equal the Python binding's."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include "tbpm_b200.h"
+int main(void) {
+  int n = 0, rc;
+  double* c = (double*)malloc(sizeof(double) * 32768);
+  printf("%d\n", tbpm_version());
+  rc = tbpm_fermi_cheb_coef(32768, 9.0 / (8.617333262e-5 * 300.0), 0.0, 1, 1e-12, c, &n);
+  printf("%d %d %.17g %.17g\n", rc, n, c[0], c[n - 1]);
+  rc = tbpm_fermi_cheb_coef(1000, 1.0, 0.0, 0, 1e-12, c, &n);
+  printf("%d\n", rc != 0);
+  free(c);
+  return 0;
+}
+""")
+    exe = tmp_path / "caller"
+    lib_dir = os.path.join(root, "tbplas_b200")
+    r = subprocess.run([cc, "-std=c99", "-O1", str(src), "-I", os.path.join(root, "include"),
+                        "-L", lib_dir, "-ltbpm_b200", "-Wl,-rpath," + lib_dir, "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    lines = out.stdout.split("\n")
+    assert int(lines[0]) > 0
+    rc, n, c0, cl = lines[1].split()
+    ref = nat.fermi_cheb_coef(2**15, 9.0 / (8.617333262e-5 * 300.0), 0.0, True, 1e-12)
+    assert int(rc) == 0 and int(n) == ref.size
+    assert float(c0) == ref[0] and float(cl) == ref[-1]
+    assert lines[2] == "1"  # a size that is not a power of two is rejected
