@@ -116,6 +116,76 @@ def test_two_rank_sample_decomposition(tmp_path):
     assert np.array_equal(res[0][3], res[1][3])
 
 
+def _worker_dc(rank, world, port, outdir, q):
+    sys.path.insert(0, ROOT)
+    try:
+        dist = _init(rank, world, port)
+        import tbplas_b200 as tb
+        from tbplas_b200.tbpm import solver as solver_mod
+        from oracle import oracle
+
+        class CpuStandIn:
+            def tbpm_dccond(self, *a):
+                return oracle.F2pyShim().tbpm_dccond(*a)
+
+            def set_backend(self, **kw):
+                pass
+
+        solver_mod.f2py = CpuStandIn()
+        s = tb.make_graphene_sample(6, 5, disorder=0.4, seed=7)
+        cfg = tb.Config()
+        cfg.generic["nr_time_steps"] = 12
+        cfg.generic["nr_random_samples"] = 3
+        cfg.DC_conductivity["energy_limits"] = (-2.0, 2.0)
+        solver = tb.Solver(s, cfg, enable_mpi=True, echo_details=False,
+                           directory=os.path.join(outdir, f"r{rank}"), prefix="d")
+        dos, dc = solver.calc_corr_dc_cond()
+        q.put((rank, dos, dc, np.isfortran(dc)))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:  # report instead of hanging the parent
+        q.put((rank, "error", repr(e), None))
+
+
+def test_two_rank_dc_conductivity(tmp_path):
+    """DC: the (n_timestep,) DOS and the (2, 2*n_timestep, n_timestep) Fortran-
+    ordered DC correlations are averaged over the ranks' samples (3 padded to
+    4), and equal the single-process oracle over the same 4 seeded samples."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_dc, args=(r, 2, port, str(tmp_path), q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(2):
+        r = q.get(timeout=240)
+        res[r[0]] = r
+    for p in procs:
+        p.join(timeout=60)
+    for r in (0, 1):
+        assert not isinstance(res[r][1], str), res[r][2]
+    assert np.array_equal(res[0][1], res[1][1]) and np.array_equal(res[0][2], res[1][2])
+    sys.path.insert(0, ROOT)
+    import math
+    import tbplas_b200 as tb
+    from oracle import oracle
+    from conftest import bessel_series
+    s = tb.make_graphene_sample(6, 5, disorder=0.4, seed=7)
+    ip, ix, hv, dx, dy = s.build_ham_dxy()
+    tnr = 12
+    en_range = s.energy_range
+    energies = np.array([0.5 * i * en_range / tnr - en_range / 2. for i in range(2 * tnr)])
+    sel = np.where((energies >= -2.0) & (energies <= 2.0))[0]
+    t_step = 2 * math.pi / en_range
+    rdos, rdc = oracle.tbpm_dccond(bessel_series(t_step * s.rescale), ip, ix, hv, s.rescale,
+                                   dx, dy, tnr, t_step, energies, sel, seed=1337, n_samples=4)
+    assert res[0][2].shape == (2, 2 * tnr, tnr)
+    assert np.max(np.abs(res[0][1] - rdos)) < 1e-13
+    assert np.max(np.abs(res[0][2] - rdc)) <= 1e-13 * max(1.0, np.max(np.abs(rdc)))
+
+
 def _worker_fail(rank, world, port, q):
     sys.path.insert(0, ROOT)
     try:
