@@ -42,6 +42,12 @@ def _init(rank, world, port, timeout_s=30):
 
 
 def _worker_solver(rank, world, port, outdir, q):
+    # one OpenMP thread per rank: two ranks share the host cores, and the oracle's
+    # small parallel regions stall on oversubscribed barriers otherwise (torch,
+    # imported with this module, has already started the OpenMP runtime)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import torch
+    torch.set_num_threads(1)
     sys.path.insert(0, ROOT)
     try:
         dist = _init(rank, world, port)
@@ -117,6 +123,12 @@ def test_two_rank_sample_decomposition(tmp_path):
 
 
 def _worker_dc(rank, world, port, outdir, q):
+    # one OpenMP thread per rank: two ranks share the host cores, and the oracle's
+    # small parallel regions stall on oversubscribed barriers otherwise (torch,
+    # imported with this module, has already started the OpenMP runtime)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import torch
+    torch.set_num_threads(1)
     sys.path.insert(0, ROOT)
     try:
         dist = _init(rank, world, port)
@@ -184,6 +196,79 @@ def test_two_rank_dc_conductivity(tmp_path):
     assert res[0][2].shape == (2, 2 * tnr, tnr)
     assert np.max(np.abs(res[0][1] - rdos)) < 1e-13
     assert np.max(np.abs(res[0][2] - rdc)) <= 1e-13 * max(1.0, np.max(np.abs(rdc)))
+
+
+def _worker_ac(rank, world, port, outdir, q):
+    # one OpenMP thread per rank: two ranks share the host cores, and the oracle's
+    # small parallel regions stall on oversubscribed barriers otherwise (torch,
+    # imported with this module, has already started the OpenMP runtime)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import torch
+    torch.set_num_threads(1)
+    sys.path.insert(0, ROOT)
+    try:
+        dist = _init(rank, world, port)
+        import tbplas_b200 as tb
+        from tbplas_b200.tbpm import solver as solver_mod
+        from oracle import oracle
+
+        class CpuStandIn:
+            def tbpm_accond(self, *a):
+                return oracle.F2pyShim().tbpm_accond(*a)
+
+            def set_backend(self, **kw):
+                pass
+
+        solver_mod.f2py = CpuStandIn()
+        s = tb.make_graphene_sample(5, 5, disorder=0.4, seed=8)
+        cfg = tb.Config()
+        cfg.generic["nr_time_steps"] = 10
+        cfg.generic["nr_random_samples"] = 2
+        solver = tb.Solver(s, cfg, enable_mpi=True, echo_details=False,
+                           directory=os.path.join(outdir, f"r{rank}"), prefix="a")
+        ac = solver.calc_corr_ac_cond()
+        q.put((rank, ac, np.isfortran(ac)))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:  # report instead of hanging the parent
+        q.put((rank, "error", repr(e)))
+
+
+def test_two_rank_ac_conductivity(tmp_path):
+    """AC: each rank propagates its own samples (Fermi operators included); the
+    (4, n_timestep) correlations averaged over the ranks equal the
+    single-process oracle over the same seeded samples."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_ac, args=(r, 2, port, str(tmp_path), q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(2):
+        r = q.get(timeout=240)
+        res[r[0]] = r
+    for p in procs:
+        p.join(timeout=60)
+    for r in (0, 1):
+        assert not isinstance(res[r][1], str), res[r][2]
+    assert np.array_equal(res[0][1], res[1][1])
+    sys.path.insert(0, ROOT)
+    import math
+    import tbplas_b200 as tb
+    from oracle import oracle
+    from conftest import bessel_series
+    s = tb.make_graphene_sample(5, 5, disorder=0.4, seed=8)
+    ip, ix, hv, dx, dy = s.build_ham_dxy()
+    cfg = tb.Config()
+    beta = cfg.generic["beta"] * s.rescale
+    mu = cfg.generic["mu"] / s.rescale
+    t_half = 0.5 * 2 * math.pi / s.energy_range
+    ref = oracle.tbpm_accond(bessel_series(t_half * s.rescale), beta, mu, ip, ix, hv, s.rescale,
+                             dx, dy, 10, seed=1337, n_samples=2)
+    assert res[0][1].shape == (4, 10) and res[0][2]
+    assert np.max(np.abs(res[0][1] - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
 
 
 def _worker_fail(rank, world, port, q):
