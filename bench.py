@@ -16,12 +16,22 @@ correlation (19 Chebyshev terms + the fused correlation) for the whole block.
   cpu_baseline  the CPU oracle (C++/OpenMP restatement of the reference
           Fortran) on this host's cores, bounded sample of the same workload
 
+  ac      the AC-conductivity time step of the same workload (48-column block
+          [J_x psi | J_y psi | psi] of the 16 states: time-step expansion +
+          the current correlations), device time per step from CUDA events
+          around two f2py.tbpm_accond calls of different lengths (their set-up,
+          Fermi operators included, cancels in the difference)
+  parity  the first two time steps of two state columns of the timed session,
+          against the CPU oracle on the same Hamiltonian and states
+
 `--impl reference` times the CPU oracle alone (the reference Fortran cannot be
 built on this image) and prints its own JSON line.
 
-Multi-GPU (torchrun): every rank propagates its own 16 states (weak scaling,
-the reference's random-sample decomposition); the correlation arrays are
-averaged with one all_reduce at the end of the e2e call.
+Multi-GPU: `--gpus N` without a torchrun environment re-launches this script
+under torch.distributed.run with N ranks (one process per GPU, NCCL).  Every
+rank propagates its own 16 states (weak scaling, the reference's random-sample
+decomposition, seeds offset by rank); the correlation arrays are averaged with
+one all_reduce at the end of the e2e call, the only data-path collective.
 """
 
 import argparse
@@ -44,9 +54,10 @@ RESCALE = 9.0
 SEED = 1337
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) over the
-# algorithmic bytes of the same launches, measured on the 1024x1024 case
-# (profiles/cheb_term_kernel_fp64_graphene.md); traffic scales with the rows.
+# algorithmic bytes of the same launches, measured with ncu on the 1024x1024
+# case of this workload; traffic scales with the rows.
 TRAFFIC_OVER_ALGORITHMIC_FP64 = 0.982
+PARITY_TOL = 1e-10
 
 
 def log(*a):
@@ -172,6 +183,118 @@ def survey_model_bytes_per_orbital_step(n, nnz, ld, n_bes, real_bytes):
     return ((n_bes - 1) * (m / (n * ld) + 5 * sv) + sv)
 
 
+def ac_algorithmic_bytes_per_step(n, nnz, nb, n_bes, real_bytes):
+    """HBM bytes of one AC time step: the time-step expansion of the
+    3*nb-column block (no correlation reference on its last term) plus the
+    current-correlation pass, which reads the CSR with hop, dx and dy once
+    and every column of the block once."""
+    ld = 3 * nb
+    sv = 2 * real_bytes
+    exp = algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes) - n * ld * sv
+    jcorr = (n + 1) * 4 + nnz * (4 + sv + 2 * real_bytes) + n * ld * sv
+    return exp + jcorr
+
+
+def free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def torchrun_command(n_gpus, port, argv):
+    """The command that runs this script as n_gpus ranks on one node."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={int(n_gpus)}", "--master-addr", "127.0.0.1",
+            f"--master-port={int(port)}", os.path.abspath(__file__)] + list(argv)
+
+
+def launch_ranks(n_gpus, argv):
+    """Re-run this script under torch.distributed.run with n_gpus ranks; NCCL
+    reports its communicators (NCCL_DEBUG=INFO) on stderr, so stdout keeps the
+    one JSON line of rank 0."""
+    env = dict(os.environ)
+    env.setdefault("NCCL_DEBUG", "INFO")
+    env.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    env.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
+    cmd = torchrun_command(n_gpus, free_port(), argv)
+    log("[bench] launching", " ".join(cmd))
+    return subprocess.call(cmd, env=env)
+
+
+def gather_rank_values(value, dist, device):
+    """(max over ranks, per-rank list) of a float, every rank taking part."""
+    import torch
+    world = dist.get_world_size()
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    parts = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(parts, t)
+    vals = [float(p.item()) for p in parts]
+    return max(vals), vals
+
+
+def parity_spot_check(ip, ix, hv, bes, corr_rows, rank, columns=(0, 1), steps=2):
+    """Relative error (max |diff| / max |oracle|) of the first `steps` time steps
+    of session columns against the CPU oracle with the same states: column b
+    of the session holds iseed = SEED * (1 + b + rank * N_STATES)."""
+    from oracle import oracle
+    n = ip.size - 1
+    worst = 0.0
+    for b in columns:
+        wf0 = oracle.random_state(n, SEED * (1 + b + rank * N_STATES), 0)
+        ref = oracle.tbpm_dos(bes, ip, ix, hv, steps, wf0=wf0, chk_step=0)
+        got = corr_rows[:steps + 1, b]
+        worst = max(worst, float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))))
+    return worst
+
+
+def time_ac(args, sample, rank, local, peak):
+    """Device time per AC time step (FP64, 16 states, 48-column block)."""
+    import torch
+    from tbplas_b200 import KB
+    from tbplas_b200.fortran import f2py
+    ip, ix, hv, dx, dy = sample.build_ham_dxy()
+    ip = ip.astype(np.int32)
+    ix = ix.astype(np.int32)
+    n, nnz = ip.size - 1, ix.size
+    bes = np.asarray(bessel_series(math.pi / 2))
+    beta = sample.rescale / (KB * 300.0)
+    G = 16
+    f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True,
+                     steps_per_graph=G, vector_width=0, threads_per_block=0)
+    ctx = f2py._ctx()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def run(tnr):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        f2py.tbpm_accond(bes, beta, 0.0, ip, ix, hv, sample.rescale, dx, dy, SEED, tnr,
+                         N_STATES, 2 ** 15, 1e-12, "unused", rank, tnr + 1, 1e-9)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
+    # t_n = 1 + (n - 1) propagated steps; both lengths replay whole graphs plus
+    # the same remainder, so capture and set-up cancel in the difference
+    short = 1 + G + 3
+    extra = G * max(1, args.ac_graphs)
+    run(short)  # warm-up (uploads, Fermi coefficients, capture)
+    t1 = run(short)
+    t2 = run(short + extra)
+    ms = (t2 - t1) / extra
+    alg = ac_algorithmic_bytes_per_step(n, nnz, N_STATES, bes.size, 8)
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"ms_per_step": ms, "orbital_steps_per_s": n * N_STATES / (ms * 1e-3),
+            "alg_bytes_per_step": alg, "achieved_gbs": gbs, "roofline_frac": gbs / peak,
+            "block_columns": 3 * N_STATES, "bessel_terms": int(bes.size),
+            "method": f"CUDA events around f2py.tbpm_accond of {short} and {short + extra} "
+                      f"time steps; ({extra} steps) / difference"}
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -183,9 +306,10 @@ def run_gpu(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     distributed = world > 1
+    torch.cuda.set_device(local)
     if distributed:
         init_distributed(backend="nccl", timeout_s=300)
-    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     peak, peak_kind = measured_peak()
 
     sample, h = build_sample()
@@ -195,18 +319,21 @@ def run_gpu(args):
     hv = np.ascontiguousarray(h.data)
     bes = np.asarray(bessel_series(2 * math.pi / sample.energy_range * sample.rescale))
     n_bes = bes.size
+    G = 16  # time steps per captured CUDA graph
 
     ctx = nat.get_context(local)
     results = {}
+    fp64_rows = None
     for prec_name, prec in (("fp64", nat.PREC_FP64), ("fp32", nat.PREC_FP32)):
         if prec_name == "fp32" and args.skip_fp32:
             continue
-        ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=16,
+        ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=G,
                         vector_width=args.vector_width if prec_name == "fp64" else 0,
                         threads_per_block=args.threads if prec_name == "fp64" else 0)
         ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, None, None,
                  sample.rescale)
         total = args.steps + args.warmup
+        # the session captures and uploads its step graph here, outside the timing
         ctx.call("tbpm_session_dos_begin", nat.ptr(bes), n_bes, N_STATES, SEED, rank, N_STATES,
                  total)
         stream = torch.cuda.ExternalStream(ctx.stream)
@@ -232,23 +359,24 @@ def run_gpu(args):
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         ms = ev0.elapsed_time(ev1)
+        per_rank = [ms]
         if distributed:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms, per_rank = gather_rank_values(ms, dist, dev)
         ms_step = ms / args.steps
         launches = (l1 - l0)
         model_bytes_step = (b1 - b0) / args.steps
         rb = 8 if prec == nat.PREC_FP64 else 4
         alg = algorithmic_bytes_per_step(n, nnz, N_STATES, n_bes, rb)
-        # parity spot check of the session against its own first rows
         corr = np.zeros((total + 1, N_STATES), dtype=np.complex128)
         norms = np.zeros((total + 1, N_STATES))
         import ctypes
         nd = ctypes.c_int(0)
         ctx.call("tbpm_session_read", nat.ptr(corr), nat.ptr(norms), ctypes.byref(nd))
+        if prec_name == "fp64":
+            fp64_rows = corr
         results[prec_name] = {
             "ms_per_step": ms_step,
+            "per_rank_ms_per_step": [v / args.steps for v in per_rank],
             "orbital_steps_per_s": n * N_STATES * world / (ms_step * 1e-3),
             "launches": launches,
             "alg_bytes_per_step": alg,
@@ -263,7 +391,8 @@ def run_gpu(args):
 
     # ---- e2e through the public API (FP64, host buffers) -----------------
     f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True,
-                     vector_width=args.vector_width, threads_per_block=args.threads)
+                     steps_per_graph=G, vector_width=args.vector_width,
+                     threads_per_block=args.threads)
     from tbplas_b200.parallel import MPIEnv
     env = MPIEnv(enable_mpi=distributed)
     e2e_steps = args.steps
@@ -276,16 +405,39 @@ def run_gpu(args):
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     if distributed:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+        t_e2e, _ = gather_rank_values(t_e2e, dist, dev)
     h2d = ip.nbytes + ix.nbytes + hv.nbytes + bes.nbytes
     d2h = corr.nbytes
     e2e = {"value": n * N_STATES * e2e_steps * world / t_e2e, "unit": "orbital-steps/s",
            "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
            "steps": e2e_steps, "seconds": t_e2e,
-           "note": "one f2py.tbpm_dos call of `steps` time steps: CSR upload and "
-                   "validation, state generation, propagation, result download"}
+           "note": "one f2py.tbpm_dos call of `steps` time steps per rank: CSR upload and "
+                   "validation, state generation, propagation, result download"
+                   + (", then the NCCL all_average of the correlation" if distributed else "")}
+
+    # ---- AC time step of the same workload (FP64) -------------------------
+    ac = None
+    if not args.skip_ac:
+        ac = time_ac(args, sample, rank, local, peak)
+        if distributed:
+            ac_ms, ac_ranks = gather_rank_values(ac["ms_per_step"], dist, dev)
+            ac["ms_per_step"] = ac_ms
+            ac["per_rank_ms_per_step"] = ac_ranks
+            ac["orbital_steps_per_s"] = n * N_STATES * world / (ac_ms * 1e-3)
+            ac["achieved_gbs"] = ac["alg_bytes_per_step"] / (ac_ms * 1e-3) / 1e9
+            ac["roofline_frac"] = ac["achieved_gbs"] / peak
+        log(f"[bench] ac fp64: {ac['ms_per_step']:.3f} ms/step, {ac['achieved_gbs']:.0f} GB/s")
+
+    # ---- parity of the timed session against the oracle -------------------
+    parity = None
+    if rank == 0 and not args.skip_parity:
+        t0 = time.perf_counter()
+        err = parity_spot_check(ip, ix, hv, bes, fp64_rows, rank)
+        parity = {"rel_err": err, "tol": PARITY_TOL, "ok": bool(err <= PARITY_TOL),
+                  "what": "FP64 session columns 0 and 1, time steps 0..2, vs the CPU oracle "
+                          "with the same states (max |diff| / max |oracle|)",
+                  "seconds": time.perf_counter() - t0}
+        log(f"[bench] parity vs oracle: {err:.3e}")
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -312,6 +464,7 @@ def run_gpu(args):
                        "n_orbitals": n, "nnz": nnz, "states_per_gpu": N_STATES,
                        "bessel_terms": n_bes, "rescale_eV": RESCALE,
                        "l2": "inputs larger than L2 (state block 2.1 GB FP64)",
+                       "steps_per_graph": G,
                        "parallelism": f"replicas of independent state blocks x{world}"},
             "roofline": {
                 "bound": "hbm",
@@ -329,9 +482,12 @@ def run_gpu(args):
             "e2e": e2e,
             "gpu_launches": int(r64["launches"]),
             "clocks": r64["clocks"],
+            "per_rank_ms_per_step": r64["per_rank_ms_per_step"],
             "fp32": {k: results["fp32"][k] for k in ("ms_per_step", "orbital_steps_per_s",
                                                       "achieved_gbs", "alg_bytes_per_step")}
             if "fp32" in results else None,
+            "ac": ac,
+            "parity": parity,
             "cpu_baseline": cpu,
         }
         if "fp32" in results:
@@ -427,6 +583,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true")
+    ap.add_argument("--skip-ac", action="store_true")
+    ap.add_argument("--skip-parity", action="store_true")
+    ap.add_argument("--ac-graphs", type=int, default=2,
+                    help="16-step graphs in the difference of the AC timing")
     ap.add_argument("--vector-width", type=int, default=0, choices=[0, 1, 2],
                     help="FP64 complex values per thread: 0 library default (two, 256-bit "
                          "accesses), 1 one (128-bit accesses), 2 two")
@@ -440,6 +600,9 @@ def main():
     NX, NY = args.nx, args.ny
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: re-run under torch.distributed.run
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     if args.impl == "reference":
         run_reference(args)
     else:

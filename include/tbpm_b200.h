@@ -354,11 +354,14 @@ int tbpm_fermi_apply(tbpm_ctx* ctx, const double* coef, int n_coef, double* wf,
  * allocator owns nearly all of HBM, or a loop where allocation after start-up
  * is forbidden.  All array arguments except bes are DEVICE pointers from the
  * caller's own allocator: the full CSR (diagonal entries included) and
- * wf = complex128 [n_rows][n_states] row-interleaved, updated in place.  The
- * two work vectors come from a fixed 16 MiB array inside the library (held by
- * every GPU that loads it until exit), so n_rows * n_states may be at most
- * 524,272; larger sizes return TBPM_ERR_ARG.  The first call on a device looks
- * up that array's device address (make it before any stream capture).  All
+ * wf = complex128 [n_rows][n_states] row-interleaved, updated in place; they
+ * must be memory of the context's device (or managed), wf and hop 16-byte
+ * aligned, indptr and indices 4-byte aligned, else TBPM_ERR_ARG before any
+ * launch.  The two work vectors come from a fixed 16 MiB array inside the
+ * library (held by every GPU that loads it until exit; 256 bytes of it are a
+ * status word), so n_rows * n_states may be at most (16 MiB - 256) / 32 =
+ * 524,280; larger sizes return TBPM_ERR_ARG.  The first call on a context
+ * looks up that array's device address (make it before any stream capture).  All
  * calls share the array: calls that overlap on the GPU race, so serialise
  * them.  The call validates the CSR on the device and is synchronous on the
  * context stream.  FP64 only. */
@@ -418,7 +421,9 @@ int tbpm_nn_cast_bf16(const float* in, int64_t n, void* out, void* stream);
 
 /* Start a DOS propagation of n_states random states (seed rule as
  * tbpm_random_states with first_sample = 1) on the uploaded Hamiltonian, with
- * room for n_timestep steps.  Records corr(0). */
+ * room for n_timestep steps.  Records corr(0).  With CUDA graphs enabled the
+ * graph of opts.steps_per_graph steps is captured and uploaded here, so that
+ * tbpm_session_advance only replays it. */
 int tbpm_session_dos_begin(tbpm_ctx* ctx, const double* bes, int n_bes, int n_states,
                            int seed, int rank, int n_ran_samples, int n_timestep);
 /* Enqueue n_steps time steps on the context stream; returns without waiting. */

@@ -62,6 +62,11 @@ class NormError(TbpmError):
     """Wave-function norm check failed (the reference Fortran `stop`s here)."""
 
 
+class NanError(NormError):
+    """The norm check found a NaN or infinite norm (TBPM_ERR_NAN); the reference's
+    check_norm treats it as a broken norm, so this is a NormError too."""
+
+
 class Options(ctypes.Structure):
     _fields_ = [
         ("precision", ctypes.c_int),
@@ -236,6 +241,8 @@ def raise_for(code: int, message: str) -> None:
         raise ValueError(message)
     if code == TBPM_ERR_NORM:
         raise NormError(code, message)
+    if code == TBPM_ERR_NAN:
+        raise NanError(code, message)
     if code == TBPM_ERR_OOM:
         raise MemoryError(message)
     raise TbpmError(code, message)

@@ -91,6 +91,8 @@ def dos_checkpointed(bes, s_indptr, s_indices, s_hop, seed, n_timestep, n_ran_sa
     """
     if every < 1:
         raise ValueError("every must be >= 1")
+    if int(n_timestep) < 1:
+        raise ValueError("n_timestep must be >= 1 for a checkpointed run")
     be = f2py.get_backend()
     bes = nat.as_c(bes, np.float64)
     ctx = f2py._ctx()
@@ -142,7 +144,11 @@ def dos_checkpointed(bes, s_indptr, s_indices, s_hop, seed, n_timestep, n_ran_sa
             chk = int(wfn_chk_step)
             if 2 <= chk <= tnr and done - k <= chk - 1 < done:
                 d = np.abs(rows_n[chk - 1] - rows_n[1])
-                if np.any(~np.isfinite(d)) or np.any(d > thr):
+                if np.any(~np.isfinite(rows_n[chk - 1])) or np.any(~np.isfinite(d)):
+                    raise nat.NanError(nat.TBPM_ERR_NAN,
+                                       f"tbpm_dos: the wave function norm is NaN or infinite "
+                                       f"at time step {chk}")
+                if np.any(d > thr):
                     raise nat.NormError(nat.TBPM_ERR_NORM,
                                         f"tbpm_dos: wave function norm gets broken during "
                                         f"propagation (time step {chk})")

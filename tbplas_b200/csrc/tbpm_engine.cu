@@ -482,6 +482,53 @@ int batch_size(const tbpm_ctx* c) {
 
 // ---- CUDA graph replay of a per-step program ---------------------------------
 
+// Capture G steps of `step` as the context's CUDA graph unless the cached one
+// has the same key and length.  The launches and modelled bytes of one step
+// are recorded with the graph (every captured step enqueues the same work),
+// so replays account for them without another capture.  The graph is also
+// uploaded to the device here, so its first launch carries no set-up work.
+template <class Fn>
+void ensure_graph(tbpm_ctx* c, const std::vector<unsigned char>& key, Fn&& step, int G) {
+  if (c->graph.exec && c->graph.key == key && c->graph.steps == G) return;
+  c->graph.reset();
+  const int64_t l0 = c->launches;
+  const double b0 = c->model_bytes;
+  TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  try {
+    for (int i = 0; i < G; ++i) step();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    c->launches = l0;
+    c->model_bytes = b0;
+    throw;
+  }
+  cudaGraph_t g = nullptr;
+  TBPM_CK(cudaStreamEndCapture(c->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&c->graph.exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->graph.exec = nullptr;
+    c->launches = l0;
+    c->model_bytes = b0;
+    throw_cuda(e, "cudaGraphInstantiate");
+  }
+  // capture does not execute: keep the per-step counts, undo the totals
+  c->graph.l_step = (c->launches - l0) / G;
+  c->graph.b_step = (c->model_bytes - b0) / G;
+  c->launches = l0;
+  c->model_bytes = b0;
+  c->graph.key = key;
+  c->graph.steps = G;
+  TBPM_CK(cudaGraphUpload(c->graph.exec, c->stream));
+}
+
+int graph_length(const tbpm_ctx* c, int graph_steps) {
+  return graph_steps > 0 ? graph_steps
+                         : (c->opts.steps_per_graph > 0 ? c->opts.steps_per_graph : 16);
+}
+
 // Enqueue n_steps of `step`: replay a CUDA graph of G captured steps as often
 // as it fits (G = graph_steps if positive, else opts.steps_per_graph), the
 // remainder directly.
@@ -489,67 +536,14 @@ template <class Fn>
 void run_steps(tbpm_ctx* c, int n_steps, const std::vector<unsigned char>& key, Fn&& step,
                int graph_steps = 0) {
   if (n_steps <= 0) return;
-  const int G = graph_steps > 0 ? graph_steps
-                                : (c->opts.steps_per_graph > 0 ? c->opts.steps_per_graph : 16);
+  const int G = graph_length(c, graph_steps);
   int done = 0;
   if (c->opts.use_graphs && n_steps >= G) {
-    if (!c->graph.exec || c->graph.key != key || c->graph.steps != G) {
-      c->graph.reset();
-      const int64_t l0 = c->launches;
-      const double b0 = c->model_bytes;
-      TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
-      try {
-        for (int i = 0; i < G; ++i) step();
-      } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(c->stream, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      cudaGraph_t g = nullptr;
-      TBPM_CK(cudaStreamEndCapture(c->stream, &g));
-      cudaError_t e = cudaGraphInstantiate(&c->graph.exec, g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) {
-        c->graph.exec = nullptr;
-        throw_cuda(e, "cudaGraphInstantiate");
-      }
-      c->graph.key = key;
-      c->graph.steps = G;
-      // capture does not execute: undo the counters recorded during capture
-      c->launches = l0;
-      c->model_bytes = b0;
-      // measure launches/bytes of one step by enqueuing nothing: recompute
-      // below from a dry count
-    }
-    // per-step launch/byte counts are identical for every replayed step
-    int64_t l_step = 0;
-    double b_step = 0;
-    {
-      const int64_t l0 = c->launches;
-      const double b0 = c->model_bytes;
-      // counting pass: run the plan builder under capture into a throwaway graph
-      TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
-      try {
-        step();
-      } catch (...) {
-        cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(c->stream, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-      }
-      cudaGraph_t g = nullptr;
-      TBPM_CK(cudaStreamEndCapture(c->stream, &g));
-      if (g) cudaGraphDestroy(g);
-      l_step = c->launches - l0;
-      b_step = c->model_bytes - b0;
-      c->launches = l0;
-      c->model_bytes = b0;
-    }
+    ensure_graph(c, key, step, G);
     while (n_steps - done >= G) {
       TBPM_CK(cudaGraphLaunch(c->graph.exec, c->stream));
-      c->launches += l_step * G;
-      c->model_bytes += b_step * G;
+      c->launches += c->graph.l_step * G;
+      c->model_bytes += c->graph.b_step * G;
       done += G;
     }
   }
@@ -596,18 +590,27 @@ double effective_thr(const tbpm_ctx* c, double thr) {
   return thr;
 }
 
-bool norm_broken(double norm, double ref, double thr) {
+// 0 when the norm passes check_norm (funcs.f90:175-192); TBPM_ERR_NAN when it
+// is NaN or infinite; TBPM_ERR_NORM when it is off the reference by more than thr.
+int norm_broken(double norm, double ref, double thr) {
   const double d = std::fabs(norm - ref);
-  return std::isnan(d) || !std::isfinite(d) || d > thr;
+  if (!std::isfinite(norm) || !std::isfinite(d)) return TBPM_ERR_NAN;
+  return d > thr ? TBPM_ERR_NORM : 0;
 }
 
-void raise_norm(const char* where, int t) {
+void raise_norm(const char* where, int t, int code) {
   char buf[320];
-  std::snprintf(buf, sizeof buf,
-                "%s: wave function norm gets broken during propagation (time step %d). "
-                "Check the Hermitianity of the Hamiltonian, then try increasing 'rescale'.",
-                where, t);
-  throw Error{TBPM_ERR_NORM, buf};
+  if (code == TBPM_ERR_NAN)
+    std::snprintf(buf, sizeof buf,
+                  "%s: the wave function norm is NaN or infinite at time step %d. Check the "
+                  "initial states and the Hamiltonian for non-finite values.",
+                  where, t);
+  else
+    std::snprintf(buf, sizeof buf,
+                  "%s: wave function norm gets broken during propagation (time step %d). "
+                  "Check the Hermitianity of the Hamiltonian, then try increasing 'rescale'.",
+                  where, t);
+  throw Error{code, buf};
 }
 
 void read_out(tbpm_ctx* c, std::vector<double>& host, size_t n_doubles) {
@@ -684,6 +687,9 @@ void dos_session_resume(tbpm_ctx* c, const Expansion& ex, int ns, const double* 
   c->sess.ex = ex;
 }
 
+// Enqueue n_steps DOS time steps of the active session; with n_steps == 0 and
+// graphs enabled, only capture (and upload) the session's step graph when
+// the session has room for at least one graph's worth of steps.
 template <typename R, int V>
 void dos_session_advance(tbpm_ctx* c, int n_steps) {
   Session& s = c->sess;
@@ -699,6 +705,12 @@ void dos_session_advance(tbpm_ctx* c, int n_steps) {
   auto step = [&]() {
     enqueue_expansion<R, V>(c, ex, ld, A, X, Y, W, ld, c->out.as<double>(), counters(c, 0));
   };
+  if (n_steps == 0) {
+    const int G = graph_length(c, 0);
+    if (c->opts.use_graphs && s.rows_cap - s.rows_enqueued >= G)
+      ensure_graph(c, plan_key(c, 1, ld, V, ex), step, G);
+    return;
+  }
   run_steps(c, n_steps, plan_key(c, 1, ld, V, ex), step);
   s.rows_enqueued += n_steps;
 }
@@ -724,7 +736,8 @@ void dos_batch(tbpm_ctx* c, const Expansion& ex, int ns, const StateKeys* keys,
     for (int b = 0; b < ns; ++b) {
       const double ref = host[((size_t)1 * ns + b) * 3 + 2];
       const double nv = host[((size_t)(chk_step - 1) * ns + b) * 3 + 2];
-      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dos", chk_step);
+      if (const int bad_ = norm_broken(nv, ref, thr))
+        raise_norm("tbpm_dos", chk_step, bad_);
     }
   }
   dos_session_advance<R, V>(c, n_timestep - done);
@@ -825,7 +838,8 @@ void dos_segmented_run(tbpm_ctx* c, const Expansion& ex, const std::vector<int64
     for (int v = 0; v < n_seg * ns; ++v) {
       const double ref = host[((size_t)1 * n_seg * ns + v) * 3 + 2];
       const double nv = host[((size_t)done * n_seg * ns + v) * 3 + 2];
-      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dos_segmented", chk_step);
+      if (const int bad_ = norm_broken(nv, ref, thr))
+        raise_norm("tbpm_dos_segmented", chk_step, bad_);
     }
     c->graph.reset();
   }
@@ -913,7 +927,8 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
     for (int b = 0; b < nb; ++b) {
       const double ref = host[(size_t)b * 9 + 8];
       const double nv = host[((size_t)done * nb + b) * 9 + 8];
-      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_accond", chk_step);
+      if (const int bad_ = norm_broken(nv, ref, thr))
+        raise_norm("tbpm_accond", chk_step, bad_);
     }
   }
   run_steps(c, (n_timestep - 1) - done, key, step);
@@ -1057,7 +1072,8 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       read_out(c, host, (size_t)(chk_step - 1) * ld * 3);
       for (int b = 0; b < ld; ++b) {
         const double nv = host[((size_t)(chk_step - 2) * ld + b) * 3 + 2];
-        if (norm_broken(nv, norm_ref[(size_t)b * 3 + 2], thr)) raise_norm(who, chk_step);
+        if (const int bad_ = norm_broken(nv, norm_ref[(size_t)b * 3 + 2], thr))
+          raise_norm(who, chk_step, bad_);
       }
     }
   }
@@ -1243,7 +1259,8 @@ void dynpol_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fer
     for (int b = 0; b < nb; ++b) {
       const double ref = host[(size_t)b * 3 + 2];
       const double nv = host[((size_t)done * tpr + b) * 3 + 2];
-      if (norm_broken(nv, ref, thr)) raise_norm("tbpm_dyn_pol", chk_step);
+      if (const int bad_ = norm_broken(nv, ref, thr))
+        raise_norm("tbpm_dyn_pol", chk_step, bad_);
     }
   }
   run_steps(c, (n_timestep - 1) - done, key, step);
@@ -1508,7 +1525,8 @@ void psi_t_run(tbpm_ctx* c, const Expansion& ex, const double* psi0, const int32
     if (t == chk_step) {
       advance_to(t - 1);
       read_out(c, host, (size_t)(done + 1) * 3);
-      if (norm_broken(host[(size_t)done * 3 + 2], host[2], thr)) raise_norm("tbpm_psi_t", t);
+      if (const int bad_ = norm_broken(host[(size_t)done * 3 + 2], host[2], thr))
+        raise_norm("tbpm_psi_t", t, bad_);
     }
   }
   if (ptr < n_log && time_log[ptr] == n_timestep) {
@@ -2291,6 +2309,8 @@ void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_stat
   dispatch(c->ham.prec, pick_V(c->ham.prec, n_states, n_states, c->opts.vector_width), [&](auto tag) {
     using P = decltype(tag);
     dos_session_begin<typename P::Real, P::V>(c, ex, n_states, &keys, nullptr, n_timestep + 1);
+    // capture the step graph now, so that the first advance only replays it
+    dos_session_advance<typename P::Real, P::V>(c, 0);
   });
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -78,6 +79,8 @@ struct GraphCache {
   cudaGraphExec_t exec = nullptr;
   std::vector<unsigned char> key;
   int steps = 0;
+  int64_t l_step = 0;   // launches of one captured step
+  double b_step = 0;    // modelled HBM bytes of one captured step
   void reset();
   ~GraphCache() { reset(); }
 };
@@ -107,4 +110,8 @@ struct tbpm_ctx {
   tbpm::Session sess;
   tbpm::GraphCache graph;
   void* blas = nullptr;  // cublasHandle_t of the Kubo-Bastin GEMMs (created on first use)
+  // device address of the allocation-free time step's fixed work array on this
+  // context's device (tbpm_noalloc.cu), looked up on its first call
+  void* noalloc_scratch = nullptr;
+  std::mutex noalloc_mutex;
 };

@@ -186,14 +186,14 @@ __global__ void __launch_bounds__(128, 1)
                     (kt > 0 || k > 0) ? 1u : 0u);
       mma_commit(&empty[s]);
     }
-    if (ok)
-      mma_commit(done);
-    else
-      failed = 1;
+    // committed on failure too: `done` then tracks every MMA already issued,
+    // so the CTA never frees its tensor memory under a running MMA
+    mma_commit(done);
+    if (!ok) failed = 1;
   }
   __syncthreads();
   bool good = !failed;
-  if (good && !mbar_wait(done, 0)) good = false;
+  if (!mbar_wait(done, 0)) good = false;
   if (!good) {
     if (tid == 0) {
       atomicExch(&g_tc_status, 1);

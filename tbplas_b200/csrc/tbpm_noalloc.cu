@@ -11,12 +11,18 @@
 // Limits and rules (also stated in include/tbpm_b200.h):
 //  * The work array holds kNoAllocScratchBytes = 16 MiB.  It is part of the
 //    library image, so every GPU that loads the library keeps it until the
-//    process exits.  It fits 2 * n_rows * n_states complex128 values with
-//    n_rows * n_states <= 524,272; larger requests are rejected with
-//    TBPM_ERR_ARG before any work is enqueued.
-//  * The first call on a device resolves the device address of the array
-//    (cudaGetSymbolAddress, with that device current) and caches it; make
-//    that first call before any stream capture.
+//    process exits.  Its first 256 bytes hold a status word; the rest fits
+//    2 * n_rows * n_states complex128 values with n_rows * n_states <=
+//    kNoAllocMaxValues = (16 MiB - 256) / 32 = 524,280; larger requests are
+//    rejected with TBPM_ERR_ARG before any work is enqueued.
+//  * The caller's arrays must be device (or managed) memory usable on the
+//    context's device, wf and hop 16-byte aligned (the kernels move them in
+//    16-byte loads) and indptr/indices 4-byte aligned; anything else is
+//    rejected on the host with TBPM_ERR_ARG before any launch.
+//  * The first call on a context resolves the device address of the array
+//    (cudaGetSymbolAddress, with the context's device current) and keeps it
+//    in the context; make that first call before any stream capture.  A
+//    context created after a cudaDeviceReset resolves it afresh.
 //  * Every call shares the one array, and it keeps the last call's contents.
 //    Calls that overlap on the GPU (other host threads, other streams) race
 //    on it: serialise them.  The status word at its start is cleared by each
@@ -38,24 +44,25 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 constexpr size_t kStatusBytes = 256;  // status word area at the start of the array
+// n_rows * n_states that the two complex128 work vectors may hold
+constexpr long long kNoAllocMaxValues =
+    (long long)((kNoAllocScratchBytes - kStatusBytes) / (2 * sizeof(double2)));
+static_assert(kNoAllocMaxValues == 524280, "documented limit of the work array");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_addr_mutex;
-void* g_addr[128] = {nullptr};
-
-// Device address of g_noalloc_scratch on `device` (must be current).  In host
+// Device address of g_noalloc_scratch for the context's device (which must be
+// current), looked up on the context's first call and kept in it.  In host
 // code the symbol name is only a host-side stand-in, never a device address.
-cudaError_t scratch_address(int device, void** out) {
-  std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (device < 0 || device >= 128) return cudaErrorInvalidDevice;
-  if (!g_addr[device]) {
+cudaError_t scratch_address(tbpm_ctx* c, void** out) {
+  std::lock_guard<std::mutex> lock(c->noalloc_mutex);
+  if (!c->noalloc_scratch) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_addr[device] = p;
+    c->noalloc_scratch = p;
   }
-  *out = g_addr[device];
+  *out = c->noalloc_scratch;
   return cudaSuccess;
 }
 
@@ -93,6 +100,29 @@ int fail_cuda(tbpm_ctx* c, cudaError_t e, const char* what) {
   return TBPM_ERR_CUDA;
 }
 
+// A caller's array: `align`-byte aligned, and device or managed memory that the
+// context's device can read (a host pointer, or another GPU's buffer, would
+// fault inside the kernels).  Queries only; nothing is allocated.
+int check_array(tbpm_ctx* c, const void* p, size_t align, const char* name) {
+  char buf[200];
+  if (reinterpret_cast<uintptr_t>(p) % align != 0) {
+    std::snprintf(buf, sizeof buf, "%s must be %zu-byte aligned", name, align);
+    return fail(c, TBPM_ERR_ARG, buf);
+  }
+  cudaPointerAttributes at{};
+  const cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) (void)cudaGetLastError();
+  const bool ok = e == cudaSuccess && (at.type == cudaMemoryTypeManaged ||
+                                       (at.type == cudaMemoryTypeDevice && at.device == c->device));
+  if (!ok) {
+    std::snprintf(buf, sizeof buf,
+                  "%s must be device (or managed) memory of the context's device %d", name,
+                  c->device);
+    return fail(c, TBPM_ERR_ARG, buf);
+  }
+  return TBPM_OK;
+}
+
 }  // namespace
 
 extern "C" int tbpm_cheb_timestep_noalloc(tbpm_ctx* c, const double* bes, int n_bes,
@@ -108,19 +138,23 @@ extern "C" int tbpm_cheb_timestep_noalloc(tbpm_ctx* c, const double* bes, int n_
     return fail(c, TBPM_ERR_ARG, "n_rows / nnz out of range");
   if (n_states < 1 || n_states > 64) return fail(c, TBPM_ERR_ARG, "n_states must be 1..64");
   const size_t vec_bytes = (size_t)n_rows * (size_t)n_states * sizeof(double2);
-  if (kStatusBytes + 2 * vec_bytes > kNoAllocScratchBytes) {
+  if ((long long)n_rows * n_states > kNoAllocMaxValues) {
     char buf[200];
     std::snprintf(buf, sizeof buf,
                   "tbpm_cheb_timestep_noalloc: n_rows*n_states = %lld exceeds the %lld "
                   "complex128 values its fixed 16 MiB work array holds",
-                  (long long)n_rows * n_states,
-                  (long long)((kNoAllocScratchBytes - kStatusBytes) / (2 * sizeof(double2))));
+                  (long long)n_rows * n_states, kNoAllocMaxValues);
     return fail(c, TBPM_ERR_ARG, buf);
   }
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return fail_cuda(c, e, "cudaSetDevice");
+  int rc = check_array(c, wf, 16, "wf");
+  if (rc == TBPM_OK) rc = check_array(c, indptr, 4, "indptr");
+  if (rc == TBPM_OK && nnz > 0) rc = check_array(c, indices, 4, "indices");
+  if (rc == TBPM_OK && nnz > 0) rc = check_array(c, hop, 16, "hop");
+  if (rc != TBPM_OK) return rc;
   void* base = nullptr;
-  e = scratch_address(c->device, &base);
+  e = scratch_address(c, &base);
   if (e != cudaSuccess) return fail_cuda(c, e, "cudaGetSymbolAddress(noalloc scratch)");
   unsigned int* status = reinterpret_cast<unsigned int*>(base);
   auto* X = reinterpret_cast<Pack<double, 1>*>(static_cast<unsigned char*>(base) + kStatusBytes);

@@ -80,7 +80,9 @@ class MPIEnv:
         arr = np.asarray(data)
         order = "F" if (arr.ndim > 1 and arr.flags.f_contiguous
                         and not arr.flags.c_contiguous) else "C"
-        flat = np.ascontiguousarray(arr.reshape(-1, order=order))
+        # a copy: the reduction must not overwrite the caller's local array
+        # (the reference's all_average reduces into a new buffer)
+        flat = np.array(arr.reshape(-1, order=order), copy=True)
         t = torch.from_numpy(flat.view(np.float64) if np.iscomplexobj(flat) else flat)
         if backend == "nccl":
             t = t.to(torch.device("cuda", torch.cuda.current_device()))

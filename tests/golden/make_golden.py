@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_golden.py --ref /root/reference --scratch /tmp/tbplas_ref
+    python tests/golden/make_golden.py --ref <reference tree> --scratch <scratch dir>
 
 The script copies the reference package to a scratch directory, compiles its
 Cython extensions there (cythonize -i), and imports it with three shims:
@@ -106,8 +106,9 @@ def sample_record(tb, out: dict, key: str, sample) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--scratch", default="/tmp/tbplas_ref_golden")
+    ap.add_argument("--ref", required=True, help="root of the reference source tree")
+    ap.add_argument("--scratch", required=True,
+                    help="scratch directory for the cythonized copy of the reference")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_tbplas.npz"))
     args = ap.parse_args()
 

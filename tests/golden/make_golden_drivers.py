@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_golden_drivers.py --ref /root/reference
+    python tests/golden/make_golden_drivers.py --ref <reference tree> --scratch <scratch dir>
 
 As make_golden.py, it imports the reference package from a scratch copy with
 the CPU oracle of this repository behind `tbplas.fortran.f2py` (the
@@ -30,8 +30,9 @@ from make_golden import install_shims, prepare_scratch  # noqa: E402
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--scratch", default="/tmp/tbplas_ref_golden")
+    ap.add_argument("--ref", required=True, help="root of the reference source tree")
+    ap.add_argument("--scratch", required=True,
+                    help="scratch directory for the cythonized copy of the reference")
     ap.add_argument("--out", default=os.path.join(HERE, "reference_drivers.npz"))
     args = ap.parse_args()
 

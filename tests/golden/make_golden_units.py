@@ -14,7 +14,7 @@ time steps:
 This script copies those arrays, unchanged, into one fixture.  Run it in a
 container that holds the reference tree:
 
-    python tests/golden/make_golden_units.py --ref /root/reference
+    python tests/golden/make_golden_units.py --ref <reference tree>
 """
 
 import argparse

@@ -368,3 +368,22 @@ def test_fp32_values_per_thread_within_bounds(dos_bes, ac_bes, driver, width):
         assert rel_err(got, ref) < 2e-5
     finally:
         f2py.set_backend(precision="fp64", vector_width=0)
+
+
+@pytest.mark.parametrize("driver", ["dos", "psi_t"])
+def test_nan_initial_state_reports_nan_status(graphene_small, dos_bes, driver):
+    """A NaN in an initial state makes every norm NaN: the norm check at
+    wfn_chk_step returns TBPM_ERR_NAN (NanError, a NormError) instead of
+    stopping the process as the reference's check_norm does."""
+    ip, ix, hv = _csr(graphene_small)
+    n = ip.size - 1
+    wf0 = unit_states(2, n, seed=3)
+    wf0[1, 7] = np.nan
+    with pytest.raises(nat.NanError, match="NaN or infinite"):
+        if driver == "dos":
+            f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0, 16, 8, 1e-9)
+        else:
+            f2py.tbpm_psi_t(dos_bes, ip, ix, hv, wf0[1], np.array([0, 4]), 16, 8, 1e-9)
+    # the context stays usable
+    got = f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0[:1], 8, 4, 1e-9)
+    assert rel_err(got, oracle.tbpm_dos(dos_bes, ip, ix, hv, 8, wf0=wf0[:1])) < FP64_TOL

@@ -1,0 +1,168 @@
+"""GPU vs oracle at sizes where every block of the persistent grid sweeps the
+rows several times.
+
+The Chebyshev-term, correlation and state kernels launch at most as many
+blocks as a B200 holds at once and walk the row tiles grid-stride.  On the
+small lattices of the other parity tests each block handles one tile, so the
+second and later sweep iterations, the per-thread accumulation of the
+correlation and norm across iterations, and the L2 prefetch of the next
+iteration's tiles would go unchecked there.  Here every case has more row
+tiles than a B200 can hold blocks (148 SMs x 2048 threads), which forces at
+least two sweep iterations whatever the occupancy, and is compared with the
+oracle on the same inputs: FP64 to a relative 1e-10 (max |diff| / max
+|oracle|), FP32 states to the stated bound.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import tbplas_b200 as tb
+from tbplas_b200.fortran import f2py
+from oracle import oracle
+
+from conftest import bessel_series, rel_err, unit_states
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 2e-5
+SMS = 148
+THREADS_PER_SM = 2048
+
+
+def max_rows_per_sweep(ld, values_per_thread, threads_wanted=128):
+    """Rows that one sweep of the largest possible persistent grid covers:
+    blocks of rpp rows x tpr threads (the library's block shape), at most
+    2048 // threads blocks per SM."""
+    tpr = ld // values_per_thread
+    rpp = max(1, threads_wanted // tpr)
+    threads = rpp * tpr
+    return SMS * (THREADS_PER_SM // threads) * rpp
+
+
+@pytest.fixture(autouse=True)
+def _backend():
+    f2py.set_backend(precision="fp64", batch=16, device=0, state_kind="exp", use_graphs=True,
+                     vector_width=0, threads_per_block=0, rows_per_tile=0)
+    yield
+    f2py.set_backend(precision="fp64", batch=16, state_kind="exp", use_graphs=True,
+                     vector_width=0)
+
+
+@pytest.fixture(scope="module")
+def g256():
+    """256 x 256 graphene cells (131,072 orbitals), W = 1 eV."""
+    return tb.make_graphene_sample(256, 256, disorder=1.0, rescale=9.0, seed=1337)
+
+
+@pytest.fixture(scope="module")
+def g128():
+    """128 x 128 graphene cells (32,768 orbitals), W = 1 eV."""
+    return tb.make_graphene_sample(128, 128, disorder=1.0, rescale=9.0, seed=11)
+
+
+def test_dos_fp64_seeded_16_states_multi_sweep(g256):
+    """16 device-generated states as one block (two complex128 per thread: 8
+    threads per row, 16 rows per 128-thread block): 8,192 row tiles."""
+    h = g256.build_ham_csr()
+    n = h.shape[0]
+    assert n > 3 * max_rows_per_sweep(16, 2)
+    bes = bessel_series(math.pi)
+    got = f2py.tbpm_dos(bes, h.indptr, h.indices, h.data, 1337, 32, 16, "unused", 0, 128, 1e-9)
+    ref = oracle.tbpm_dos(bes, h.indptr, h.indices, h.data, 32, seed=1337, n_samples=16)
+    assert rel_err(got, ref) < FP64_TOL
+
+
+def test_dos_fp32_16_states_multi_sweep(g256):
+    """FP32 states, four complex64 per thread (4 threads per row)."""
+    h = g256.build_ham_csr()
+    n = h.shape[0]
+    assert n > max_rows_per_sweep(16, 4)
+    wf0 = unit_states(16, n, seed=5)
+    bes = bessel_series(math.pi)
+    f2py.set_backend(precision="fp32")
+    got = f2py.tbpm_dos_states(bes, h.indptr, h.indices, h.data, wf0, 32, 16, 1e-9)
+    ref = oracle.tbpm_dos(bes, h.indptr, h.indices, h.data, 32, wf0=wf0)
+    assert rel_err(got, ref) < FP32_TOL
+
+
+def test_ac_fp64_48_column_block_multi_sweep(g128):
+    """16 states: the AC block [J_x psi | J_y psi | psi] has 48 columns (24
+    threads per row, 5 rows per 120-thread block: 6,554 row tiles).  The Fermi
+    operator is taken at 3000 K, which shortens its expansion; the kernels are
+    the same as at 300 K."""
+    ip, ix, hv, dx, dy = g128.build_ham_dxy()
+    n = ip.size - 1
+    assert n > 2 * max_rows_per_sweep(48, 2)
+    wf0 = unit_states(16, n, seed=21)
+    bes = bessel_series(math.pi / 2)
+    beta = g128.rescale / (tb.KB * 3000.0)
+    got = f2py.tbpm_accond_states(bes, beta, 0.0, ip, ix, hv, g128.rescale, dx, dy, wf0, 12,
+                                  2**15, 1e-12, 128, 1e-9)
+    ref = oracle.tbpm_accond(bes, beta, 0.0, ip, ix, hv, g128.rescale, dx, dy, 12, wf0=wf0)
+    assert np.all(got[:, 0] == 0)
+    assert rel_err(got, ref) < FP64_TOL
+
+
+def test_dc_fp64_16_states_two_energy_chunks_multi_sweep(g128):
+    """16 states (a 32-column +/- block, 8 rows per block) and 44 energies: the
+    quasi-eigenstate kernels cover 32 energies x 16 states per block row, so
+    each row takes two element chunks."""
+    ip, ix, hv, dx, dy = g128.build_ham_dxy()
+    n = ip.size - 1
+    assert n > max_rows_per_sweep(32, 2)
+    tnr = 24
+    en_range = g128.energy_range
+    energies = np.array([0.5 * i * en_range / tnr - en_range / 2. for i in range(2 * tnr)])
+    sel = np.where((energies >= -8.0) & (energies <= 8.0))[0]
+    assert sel.size > 32
+    wf0 = unit_states(16, n, seed=31)
+    bes = bessel_series(math.pi)
+    t_step = 2 * math.pi / en_range
+    dos, dc = f2py.tbpm_dccond_states(bes, ip, ix, hv, g128.rescale, dx, dy, wf0, tnr, t_step,
+                                      energies, sel, 128, 1e-9)
+    rdos, rdc = oracle.tbpm_dccond(bes, ip, ix, hv, g128.rescale, dx, dy, tnr, t_step,
+                                   energies, sel, wf0=wf0)
+    assert rel_err(dos, rdos) < FP64_TOL
+    assert rel_err(dc, rdc) < FP64_TOL
+
+
+def test_psi_t_fp64_one_state_multi_sweep():
+    """One state (one thread per row, 128 rows per block) of 512 x 512 graphene
+    (524,288 orbitals)."""
+    s = tb.make_graphene_sample(512, 512, disorder=1.0, rescale=9.0, seed=41)
+    h = s.build_ham_csr()
+    n = h.shape[0]
+    assert n > max_rows_per_sweep(1, 1)
+    psi0 = unit_states(1, n, seed=43)[0]
+    bes = bessel_series(math.pi)
+    time_log = np.array([0, 1, 7, 12])
+    got = f2py.tbpm_psi_t(bes, h.indptr, h.indices, h.data, psi0, time_log, 12, 128, 1e-9)
+    ref = oracle.tbpm_psi_t(bes, h.indptr, h.indices, h.data, psi0, time_log, 12)
+    assert rel_err(got, ref) < FP64_TOL
+    assert np.allclose(np.linalg.norm(got, axis=0), 1.0, atol=1e-12)
+
+
+def test_cheb_timestep_multi_sweep(g256):
+    """The allocating time-step entry point on 16 states, forward then back."""
+    from tbplas_b200 import _native as nat
+    h = g256.build_ham_csr()
+    n = h.shape[0]
+    wf = unit_states(16, n, seed=17)
+    ctx = f2py._ctx()
+    ip32, ix32 = h.indptr.astype(np.int32), h.indices.astype(np.int32)
+    hv = np.ascontiguousarray(h.data)
+    ctx.call("tbpm_ham_upload", nat.ptr(ip32), nat.ptr(ix32), nat.ptr(hv), n, hv.size, None,
+             None, 1.0)
+    bes = np.asarray(bessel_series(math.pi))
+    got = np.ascontiguousarray(wf.copy())
+    ctx.call("tbpm_cheb_timestep", nat.ptr(bes), bes.size, nat.ptr(got), 16, 1)
+    ref = np.stack([oracle.cheb_timestep(bes, h.indptr, h.indices, h.data, wf[b])
+                    for b in range(16)])
+    assert rel_err(got, ref) < 1e-12
+    ctx.call("tbpm_cheb_timestep", nat.ptr(bes), bes.size, nat.ptr(got), 16, 0)
+    back = np.stack([oracle.cheb_timestep(bes, h.indptr, h.indices, h.data, ref[b],
+                                          forward=False) for b in range(16)])
+    assert rel_err(got, back) < 1e-12

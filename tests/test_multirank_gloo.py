@@ -69,7 +69,9 @@ def _worker_solver(rank, world, port, outdir, q):
         env = MPIEnv(enable_mpi=True)
         x = np.asfortranarray(np.arange(6, dtype=np.complex128).reshape(2, 3) * (rank + 1)
                               + 1j * rank)
-        avg = env.all_average(x.copy(order="F"))
+        xl = x.copy(order="F")
+        avg = env.all_average(xl)
+        untouched = bool(np.array_equal(xl, x))  # the local array keeps its values
         b = np.full(4, float(rank))
         env.bcast(b)
         s = tb.make_graphene_sample(6, 6, disorder=0.5, seed=3)
@@ -79,11 +81,11 @@ def _worker_solver(rank, world, port, outdir, q):
         solver = tb.Solver(s, cfg, enable_mpi=True, echo_details=False,
                            directory=os.path.join(outdir, f"r{rank}"), prefix="m")
         corr = solver.calc_corr_dos()
-        q.put((rank, avg, b, corr, cfg.generic["nr_random_samples"]))
+        q.put((rank, avg, b, corr, cfg.generic["nr_random_samples"], untouched))
         dist.barrier()
         dist.destroy_process_group()
     except Exception as e:  # report instead of hanging the parent
-        q.put((rank, "error", repr(e), None, None))
+        q.put((rank, "error", repr(e), None, None, None))
 
 
 def test_two_rank_sample_decomposition(tmp_path):
@@ -105,8 +107,9 @@ def test_two_rank_sample_decomposition(tmp_path):
     x0 = np.arange(6, dtype=np.complex128).reshape(2, 3)
     expect = (x0 * 1 + x0 * 2 + 1j) / 2
     for r in (0, 1):
-        _, avg, b, corr, nrs = res[r]
+        _, avg, b, corr, nrs, untouched = res[r]
         assert np.allclose(avg, expect)
+        assert untouched
         assert np.all(b == 0.0)
         assert nrs == 4  # padded to a multiple of the number of ranks
     sys.path.insert(0, ROOT)

@@ -183,3 +183,26 @@ int main(void) {
     assert int(rc) == 0 and int(n) == ref.size
     assert float(c0) == ref[0] and float(cl) == ref[-1]
     assert lines[2] == "1"  # a size that is not a power of two is rejected
+
+
+def test_status_codes_map_to_python_errors():
+    """TBPM_ERR_NAN becomes NanError, which callers that catch the reference's
+    broken-norm failure (NormError) also catch."""
+    with pytest.raises(nat.NanError) as e:
+        nat.raise_for(nat.TBPM_ERR_NAN, "tbpm_dos: the wave function norm is NaN")
+    assert isinstance(e.value, nat.NormError) and e.value.code == nat.TBPM_ERR_NAN
+    with pytest.raises(nat.NormError) as e:
+        nat.raise_for(nat.TBPM_ERR_NORM, "broken")
+    assert not isinstance(e.value, nat.NanError)
+    with pytest.raises(ValueError):
+        nat.raise_for(nat.TBPM_ERR_ARG, "bad")
+
+
+def test_checkpointed_run_rejects_zero_steps(tmp_path):
+    from tbplas_b200.checkpoint import dos_checkpointed
+    ip = np.array([0, 1, 2], dtype=np.int32)
+    ix = np.array([1, 0], dtype=np.int32)
+    hv = np.ones(2, dtype=np.complex128)
+    with pytest.raises(ValueError, match="n_timestep"):
+        dos_checkpointed([1.0, 0.5, 0.1], ip, ix, hv, 1337, 0, 1, 0, 128, 1e-9,
+                         str(tmp_path / "c.npz"))
