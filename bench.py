@@ -263,7 +263,8 @@ def time_ac(args, sample, rank, local, peak):
     beta = sample.rescale / (KB * 300.0)
     G = 16
     f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True,
-                     steps_per_graph=G, vector_width=0, threads_per_block=0)
+                     steps_per_graph=G, vector_width=0, threads_per_block=0,
+                     term_kernel=args.term_kernel)
     ctx = f2py._ctx()
     stream = torch.cuda.ExternalStream(ctx.stream)
 
@@ -329,7 +330,8 @@ def run_gpu(args):
             continue
         ctx.set_options(precision=prec, batch=N_STATES, use_graphs=1, steps_per_graph=G,
                         vector_width=args.vector_width if prec_name == "fp64" else 0,
-                        threads_per_block=args.threads if prec_name == "fp64" else 0)
+                        threads_per_block=args.threads if prec_name == "fp64" else 0,
+                        term_kernel=args.term_kernel)
         ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, None, None,
                  sample.rescale)
         total = args.steps + args.warmup
@@ -392,7 +394,7 @@ def run_gpu(args):
     # ---- e2e through the public API (FP64, host buffers) -----------------
     f2py.set_backend(precision="fp64", batch=N_STATES, device=local, use_graphs=True,
                      steps_per_graph=G, vector_width=args.vector_width,
-                     threads_per_block=args.threads)
+                     threads_per_block=args.threads, term_kernel=args.term_kernel)
     from tbplas_b200.parallel import MPIEnv
     env = MPIEnv(enable_mpi=distributed)
     e2e_steps = args.steps
@@ -590,6 +592,9 @@ def main():
     ap.add_argument("--vector-width", type=int, default=0, choices=[0, 1, 2],
                     help="FP64 complex values per thread: 0 library default (two, 256-bit "
                          "accesses), 1 one (128-bit accesses), 2 two")
+    ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="Chebyshev-term kernel: 0 library default (shared-memory ring fed by "
+                         "bulk copies), 1 grid-stride kernel with plain loads, 2 ring")
     ap.add_argument("--threads", type=int, default=0,
                     help="FP64 threads per block of the term kernel (0: library default)")
     ap.add_argument("--nx", type=int, default=2048,

@@ -79,6 +79,8 @@ class Options(ctypes.Structure):
         ("use_graphs", ctypes.c_int),
         ("fp32_chk_thr", ctypes.c_double),
         ("vector_width", ctypes.c_int),
+        ("term_kernel", ctypes.c_int),
+        ("dc_budget_gb", ctypes.c_double),
     ]
 
 

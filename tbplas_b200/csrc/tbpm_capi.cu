@@ -56,7 +56,6 @@ void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
               int n_ran_samples, int n_kernel, int direction, double* mu);
 void drv_haydock(tbpm_ctx* c, const int32_t* sites, int n_sites, const double* wf_sites,
                  int n_samples, int n_depth, double h_rescale, double* coefa, double* coefb);
-void release_blas(tbpm_ctx* c);
 void drv_cond_from_trace(tbpm_ctx* c, const double* mu_mn, int nk, const double* mu, int n_mu,
                          double h_rescale, double beta, int ne_integral, double* cond);
 void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
@@ -80,6 +79,8 @@ tbpm_options default_options() {
   o.use_graphs = 1;
   o.fp32_chk_thr = 1e-4;
   o.vector_width = 0;
+  o.term_kernel = 0;
+  o.dc_budget_gb = 0.0;
   return o;
 }
 
@@ -135,6 +136,20 @@ int tbpm_create(int device, tbpm_ctx** out) {
     delete c;
     return TBPM_ERR_CUDA;
   }
+  // status word of the kernels' bounded waits (zero = no wait ran out)
+  try {
+    c->status.ensure(256);
+  } catch (...) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return TBPM_ERR_OOM;
+  }
+  if (cudaMemset(c->status.p, 0, 256) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return TBPM_ERR_CUDA;
+  }
   *out = c;
   return TBPM_OK;
 }
@@ -150,7 +165,6 @@ int tbpm_destroy(tbpm_ctx* c) {
   c->ham.dx.release();
   c->ham.dy.release();
   c->ham.diag.release();
-  tbpm::release_blas(c);
   cudaStreamDestroy(c->stream);
   delete c;
   return TBPM_OK;
@@ -170,7 +184,8 @@ int tbpm_set_options(tbpm_ctx* c, const tbpm_options* o) {
   }
   if (o->batch < 0 || o->threads_per_block < 0 || o->rows_per_tile < 0 ||
       o->steps_per_graph < 0 || !(o->fp32_chk_thr >= 0) || o->vector_width < 0 ||
-      o->vector_width > 2) {
+      o->vector_width > 2 || o->term_kernel < 0 || o->term_kernel > 2 ||
+      !(o->dc_budget_gb >= 0)) {
     c->err = "negative option";
     return TBPM_ERR_ARG;
   }

@@ -22,11 +22,12 @@
 #include "tbpm_dc_kernels.cuh"
 #include "tbpm_seg_kernels.cuh"
 #include "tbpm_kernels.cuh"
+#include "tbpm_ring_kernels.cuh"
+#include "tbpm_pq_gemm.cuh"
+#include "tbpm_ring_kernels.cuh"
 #include "tbpm_more_kernels.cuh"
 #include "tbpm_scan.cuh"
 
-#include <cublas_v2.h>
-#include <dlfcn.h>
 
 namespace tbpm {
 
@@ -40,6 +41,7 @@ void DevMem::ensure(size_t n) {
   if (n <= bytes && p) return;
   release();
   if (n == 0) n = 16;
+  n = (n + 255) & ~(size_t)255;
   TBPM_CK(cudaMalloc(&p, n));
   bytes = n;
 }
@@ -244,10 +246,77 @@ void ensure_partials(tbpm_ctx* c, size_t n_doubles) {
   c->partials.ensure(std::max(n_doubles, floor_doubles) * sizeof(double));
 }
 
-// Launch shapes of the three compiled modes of cheb_term_kernel.
+// Launch shapes of the three compiled modes of the Chebyshev-term kernel, and
+// for each mode whether the shared-memory ring kernel runs it.
 struct TermTiles {
   Tile t[3];
+  bool ring[3] = {false, false, false};
+  RingShape rs[3] = {};
 };
+
+// Ring layout for rows of tpr packs in kernel mode `mode`; stages == 0 when the
+// ring does not apply (rows that are not a multiple of 16 bytes, or a stage
+// that does not fit twice into half of an SM's shared memory).
+template <typename R, int V>
+RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode) {
+  RingShape s{};
+  const size_t row_bytes = (size_t)tpr * sizeof(Pack<R, V>);
+  if (row_bytes % 16 != 0 || tpr < 1 || tpr > kRingConsumers) return s;
+  const int TR = kRingConsumers / tpr;
+  const Ham& h = c->ham;
+  const size_t cs = sizeof(typename Cx<R>::t);
+  // CSR entries one stage holds: the mean row length of O over a tile with 25%
+  // slack, plus the widening to 16-byte boundaries; denser tiles read their
+  // entries from global memory instead
+  const double per_row = h.n > 0 ? (double)h.nnz / (double)h.n : 0.0;
+  int cap = (int)std::ceil(per_row * TR * 1.25) + 8;
+  cap = (cap + 3) & ~3;
+  auto al = [](size_t b) { return (int)((b + 127) & ~(size_t)127); };
+  const int tile = al((size_t)TR * row_bytes);
+  int off = 0;
+  s.pin_off = off;
+  off += tile;
+  s.own_off = off;
+  off += tile;
+  s.acc_off = -1;
+  if (mode >= 1) {
+    s.acc_off = off;
+    off += tile;
+  }
+  s.diag_off = off;
+  off += al((size_t)(TR + 2) * cs);
+  s.ip_off = off;
+  off += al((size_t)(TR + 8) * 4);
+  s.ix_off = off;
+  off += al((size_t)cap * 4);
+  s.hop_off = off;
+  off += al((size_t)cap * cs);
+  s.stage_bytes = off;
+  // two resident blocks per SM (228 KB of shared memory, 1 KB reserved per block)
+  const int budget = (228 * 1024) / 2 - 1024 - 256;
+  const int S = std::min(kRingMaxStages, budget / off);
+  if (S < 2) return RingShape{};
+  s.rows = TR;
+  s.stages = S;
+  s.cap = cap;
+  s.bar_off = S * off;
+  s.smem_bytes = s.bar_off + 2 * S * 8;
+  // MODE 2 reduces its partials in the stage buffers
+  if ((size_t)s.bar_off < (size_t)kRingConsumers * V * 3 * sizeof(double)) return RingShape{};
+  return s;
+}
+
+template <typename R, int V, int MODE>
+int ring_blocks_per_sm(const tbpm_ctx* c, const RingShape& rs) {
+  static bool attr_set[64] = {false};
+  const int dev = c->device;
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    TBPM_CK(cudaFuncSetAttribute(cheb_ring_kernel<R, V, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set[dev] = true;
+  }
+  return resident_per_sm(cheb_ring_kernel<R, V, MODE>, kRingThreads, (size_t)rs.smem_bytes);
+}
 
 #ifndef TBPM_F32V4_THREADS
 #define TBPM_F32V4_THREADS 128
@@ -261,6 +330,25 @@ TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr) {
   tt.t[0] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 0>, 0, th);
   tt.t[1] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 1>, 0, th);
   tt.t[2] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 2>, V * 3 * sizeof(double), th);
+  if (c->opts.term_kernel != 1) {
+    for (int m = 0; m < 3; ++m) {
+      const RingShape rs = ring_shape<R, V>(c, tpr, m);
+      if (rs.stages == 0) continue;
+      const int per_sm = m == 0   ? ring_blocks_per_sm<R, V, 0>(c, rs)
+                         : m == 1 ? ring_blocks_per_sm<R, V, 1>(c, rs)
+                                  : ring_blocks_per_sm<R, V, 2>(c, rs);
+      const int64_t tiles = (n_rows + rs.rows - 1) / rs.rows;
+      Tile t;
+      t.threads = kRingThreads;
+      t.rpp = rs.rows;
+      t.rows_per_tile = rs.rows;
+      t.grid = (int)std::max<int64_t>(
+          1, std::min<int64_t>((int64_t)per_sm * num_sms(c->device), tiles));
+      tt.t[m] = t;
+      tt.ring[m] = true;
+      tt.rs[m] = rs;
+    }
+  }
   return tt;
 }
 
@@ -269,7 +357,19 @@ template <typename R, int V>
 int launch_term(tbpm_ctx* c, const TermTiles& tt, const TermArgs<R, V>& a) {
   const int mode = a.partials ? 2 : (a.c.nflush > 0 ? 1 : 0);
   const Tile& t = tt.t[mode];
-  if (mode == 2) {
+  if (tt.ring[mode]) {
+    RingArgs<R, V> ra;
+    ra.t = a;
+    ra.s = tt.rs[mode];
+    ra.status = c->status.as<unsigned int>();
+    const size_t smem = (size_t)ra.s.smem_bytes;
+    if (mode == 2)
+      cheb_ring_kernel<R, V, 2><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    else if (mode == 1)
+      cheb_ring_kernel<R, V, 1><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    else
+      cheb_ring_kernel<R, V, 0><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+  } else if (mode == 2) {
     const size_t smem = (size_t)t.threads * V * 3 * sizeof(double);
     cheb_term_kernel<R, V, 2><<<t.grid, t.threads, smem, c->stream>>>(a);
   } else if (mode == 1) {
@@ -415,6 +515,8 @@ void upload_states(tbpm_ctx* c, const double* host, int ns, int ld, int col0, vo
   c->launches++;
 }
 
+void check_status(tbpm_ctx* c);
+
 // Columns [col0, col0+ns) of src -> host complex128 [ns][n] (synchronous).
 template <typename R>
 void download_states(tbpm_ctx* c, const void* src, int ns, int ld, int col0, double* host) {
@@ -427,6 +529,7 @@ void download_states(tbpm_ctx* c, const void* src, int ns, int ld, int col0, dou
   c->launches++;
   TBPM_CK(cudaMemcpyAsync(host, c->stage.p, bytes, cudaMemcpyDeviceToHost, c->stream));
   TBPM_CK(cudaStreamSynchronize(c->stream));
+  check_status(c);
 }
 
 void ensure_vectors(tbpm_ctx* c, int ld, int ref_ld) {
@@ -613,9 +716,23 @@ void raise_norm(const char* where, int t, int code) {
   throw Error{code, buf};
 }
 
+// After a synchronisation: TBPM_ERR_TIMEOUT if a bounded wait of a kernel ran
+// out since the last check (the word is cleared).
+void check_status(tbpm_ctx* c) {
+  unsigned int st = 0;
+  TBPM_CK(cudaMemcpy(&st, c->status.p, sizeof st, cudaMemcpyDeviceToHost));
+  if (st) {
+    TBPM_CK(cudaMemset(c->status.p, 0, sizeof st));
+    throw Error{TBPM_ERR_TIMEOUT,
+                "a bounded device-side wait of a Chebyshev-term kernel ran out; the results "
+                "of this call are invalid"};
+  }
+}
+
 void read_out(tbpm_ctx* c, std::vector<double>& host, size_t n_doubles) {
   host.resize(n_doubles);
   TBPM_CK(cudaStreamSynchronize(c->stream));
+  check_status(c);
   if (n_doubles)
     TBPM_CK(cudaMemcpy(host.data(), c->out.p, n_doubles * sizeof(double), cudaMemcpyDeviceToHost));
 }
@@ -973,7 +1090,7 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
               const StateKeys* keys, const double* host_wf0, int n_timestep, double t_step,
               const std::vector<double>& en_sel, int chk_step, double chk_thr, int n_avg,
               int n_energies, double* dos_corr, double* dc_corr, double* qe_acc = nullptr,
-              const char* who = "tbpm_dccond") {
+              const char* who = "tbpm_dccond", int en_out0 = 0, bool add_dos = true) {
   using C = typename Cx<R>::t;
   const Ham& h = c->ham;
   const int64_t n = h.n;
@@ -1101,11 +1218,12 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
     return;
   }
   read_out(c, host, (size_t)n_timestep * ld * 3);
-  for (int b = 0; b < nb; ++b)
-    for (int tt = 1; tt <= n_timestep; ++tt) {
-      dos_corr[2 * (tt - 1)] += host[((size_t)(tt - 1) * ld + b) * 3 + 0] / n_avg;
-      dos_corr[2 * (tt - 1) + 1] += host[((size_t)(tt - 1) * ld + b) * 3 + 1] / n_avg;
-    }
+  if (add_dos)
+    for (int b = 0; b < nb; ++b)
+      for (int tt = 1; tt <= n_timestep; ++tt) {
+        dos_corr[2 * (tt - 1)] += host[((size_t)(tt - 1) * ld + b) * 3 + 0] / n_avg;
+        dos_corr[2 * (tt - 1) + 1] += host[((size_t)(tt - 1) * ld + b) * 3 + 1] / n_avg;
+      }
   if (n_en == 0) return;
   // ---- phase 2 ----
   const int n_ib = n_en * nb;
@@ -1184,7 +1302,8 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
             const int ib = i * nb + b;
             const int64_t o = ((int64_t)(tau * 2 + k) * n_ib + ib) * 2;
             const double a = amp[ib];
-            const size_t d = 2 * ((size_t)k + 2 * ((size_t)i + (size_t)n_energies * (t + tau - 1)));
+            const size_t d = 2 * ((size_t)k + 2 * ((size_t)(en_out0 + i) +
+                                                   (size_t)n_energies * (t + tau - 1)));
             dc_corr[d] += vals[o] / a / n_avg;
             dc_corr[d + 1] += vals[o + 1] / a / n_avg;
           }
@@ -1274,57 +1393,6 @@ void dynpol_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fer
 
 // ---- Kubo-Bastin mu_mn ------------------------------------------------------------
 
-// cuBLAS is bound at first use (dlopen), so loading the library does not pull
-// it in for drivers that do not need it.
-struct BlasApi {
-  bool ok = false;
-  decltype(&cublasCreate_v2) create = nullptr;
-  decltype(&cublasSetStream_v2) set_stream = nullptr;
-  decltype(&cublasZgemm_v2) zgemm = nullptr;
-  decltype(&cublasCgemm_v2) cgemm = nullptr;
-  decltype(&cublasDestroy_v2) destroy = nullptr;
-};
-
-const BlasApi& blas_api() {
-  static BlasApi api = [] {
-    BlasApi a;
-    void* lib = dlopen("libcublas.so.12", RTLD_NOW | RTLD_LOCAL);
-    if (!lib) lib = dlopen("libcublas.so", RTLD_NOW | RTLD_LOCAL);
-    if (!lib) return a;
-    a.create = reinterpret_cast<decltype(a.create)>(dlsym(lib, "cublasCreate_v2"));
-    a.set_stream = reinterpret_cast<decltype(a.set_stream)>(dlsym(lib, "cublasSetStream_v2"));
-    a.zgemm = reinterpret_cast<decltype(a.zgemm)>(dlsym(lib, "cublasZgemm_v2"));
-    a.cgemm = reinterpret_cast<decltype(a.cgemm)>(dlsym(lib, "cublasCgemm_v2"));
-    a.destroy = reinterpret_cast<decltype(a.destroy)>(dlsym(lib, "cublasDestroy_v2"));
-    a.ok = a.create && a.set_stream && a.zgemm && a.cgemm && a.destroy;
-    return a;
-  }();
-  return api;
-}
-
-template <typename R>
-struct Blas;
-template <>
-struct Blas<double> {
-  using T = cuDoubleComplex;
-  static cublasStatus_t gemm(cublasHandle_t h, int m, int n, int k, const void* A, int lda,
-                             const void* B, int ldb, void* C, int ldc) {
-    const T one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-    return blas_api().zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, n, k, &one, (const T*)A, lda,
-                            (const T*)B, ldb, &zero, (T*)C, ldc);
-  }
-};
-template <>
-struct Blas<float> {
-  using T = cuComplex;
-  static cublasStatus_t gemm(cublasHandle_t h, int m, int n, int k, const void* A, int lda,
-                             const void* B, int ldb, void* C, int ldc) {
-    const T one = make_cuComplex(1.0f, 0.0f), zero = make_cuComplex(0.0f, 0.0f);
-    return blas_api().cgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, n, k, &one, (const T*)A, lda,
-                            (const T*)B, ldb, &zero, (T*)C, ldc);
-  }
-};
-
 // scatter site amplitudes into a zeroed vector (tbpm.f90:1005-1008)
 template <typename R>
 __global__ void scatter_sites_kernel(const int32_t* sites, const double2* vals, int n_sites,
@@ -1337,28 +1405,31 @@ __global__ void scatter_sites_kernel(const int32_t* sites, const double2* vals, 
   v[sites[i]] = o;
 }
 
-// mu[i + nk*j] += g_i g_j Cs[i + kc*j... ] / n_avg for the rows i0..i0+kc of a chunk
-template <typename R>
-__global__ void mu_accum_kernel(const typename Cx<R>::t* cs, int kc, int nk, int i0,
-                                const double* g, double scale, double2* mu) {
-  const int64_t total = (int64_t)kc * nk;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int ii = (int)(e % kc);
-    const int j = (int)(e / kc);
-    const int i = i0 + ii;
-    const typename Cx<R>::t v = cs[e];
-    const double w = g[i] * g[j];
-    double2& m = mu[(int64_t)i + (int64_t)nk * j];
-    m.x += w * (double)v.x * scale;
-    m.y += w * (double)v.y * scale;
-  }
+// Slices of the N rows for the split-K contraction: enough blocks for about
+// four per SM, slices a multiple of the 16-row step.
+struct PqSplit {
+  int slices;
+  int64_t rows;
+};
+
+PqSplit pq_split(const tbpm_ctx* c, int64_t n, int m, int nk) {
+  const int64_t tiles = (int64_t)((m + kPqTile - 1) / kPqTile) * ((nk + kPqTile - 1) / kPqTile);
+  const int64_t want = std::max<int64_t>(1, (4 * (int64_t)num_sms(c->device) + tiles - 1) / tiles);
+  const int64_t max_slices = std::max<int64_t>(1, n / (16 * kPqK));
+  const int64_t sl = std::min(want, max_slices);
+  int64_t rows = (n + sl - 1) / sl;
+  rows = (rows + kPqK - 1) / kPqK * kPqK;
+  PqSplit p;
+  p.rows = rows;
+  p.slices = (int)((n + rows - 1) / rows);
+  return p;
 }
 
 // One state of tbpm_kbdc (tbpm.f90:898-957).  Q holds J_a T_j(H) psi for all
 // j (N x nk, column-major); the bra vectors T_i(H) J_x psi are generated in
-// chunks of kc columns and contracted with Q by one complex GEMM per chunk:
-// the nk^2 inner products of the reference as a (kc x N) . (N x nk) product.
+// chunks of kc columns and contracted with Q by one complex GEMM per chunk
+// (pq_gemm_kernel, split over N, and pq_reduce_kernel): the nk^2 inner
+// products of the reference as a (kc x N) . (N x nk) product.
 template <typename R>
 void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double scale,
                 double2* mu_dev) {
@@ -1371,7 +1442,7 @@ void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double 
   C* P = c->X.as<C>();
   C* ring = c->Y.as<C>();  // 5 vectors: T ring (3) and the P carry (2)
   C* psi = c->wf0.as<C>();
-  C* cs = reinterpret_cast<C*>(c->qe.as<char>());
+  double2* ws = c->qe.as<double2>();  // split partials of the contraction
   const int grid = (int)std::min<int64_t>(blocks_for(n, 256), (int64_t)kSMs * 16);
   const C* diag = h.has_diag ? h.diag.as<C>() : nullptr;
   const R* dj = direction == 1 ? h.dx.as<R>() : h.dy.as<R>();
@@ -1400,7 +1471,6 @@ void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double 
   }
   // bra side in chunks: P_i = T_i(H) J_x psi, then mu[i0:i0+kc, :] += P^H Q
   C* carry[2] = {ring + 3 * n, ring + 4 * n};
-  cublasHandle_t bh = reinterpret_cast<cublasHandle_t>(c->blas);
   for (int i0 = 0; i0 < nk; i0 += kc) {
     const int m = std::min(kc, nk - i0);
     for (int ii = 0; ii < m; ++ii) {
@@ -1416,10 +1486,13 @@ void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double 
       else
         hmv(2.0, -1.0, pm1, pm2, pi);  // p_i = 2 H p_i-1 - p_i-2 (:950)
     }
-    if (Blas<R>::gemm(bh, m, nk, (int)n, P, (int)n, Q, (int)n, cs, m) != CUBLAS_STATUS_SUCCESS)
-      throw Error{TBPM_ERR_CUDA, "complex GEMM of the Kubo-Bastin moments failed"};
-    mu_accum_kernel<R><<<(int)std::min<int64_t>(blocks_for((int64_t)m * nk, 256), 4096), 256, 0,
-                         c->stream>>>(cs, m, nk, i0, g_dev, scale, mu_dev);
+    const PqSplit sp = pq_split(c, n, m, nk);
+    pq_gemm_kernel<R><<<dim3((nk + kPqTile - 1) / kPqTile, (m + kPqTile - 1) / kPqTile,
+                             sp.slices),
+                        256, 0, c->stream>>>(P, Q, n, m, nk, sp.rows, ws);
+    TBPM_CK(cudaGetLastError());
+    pq_reduce_kernel<<<(int)std::min<int64_t>(blocks_for((int64_t)m * nk, 256), 4096), 256, 0,
+                       c->stream>>>(ws, sp.slices, m, nk, i0, g_dev, scale, mu_dev);
     TBPM_CK(cudaGetLastError());
     c->launches += 2;
     // carry the last two bra vectors into the next chunk
@@ -1873,20 +1946,38 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
   std::fill(dos_corr, dos_corr + 2 * (size_t)n_timestep, 0.0);
   std::fill(dc_corr, dc_corr + 2 * 2 * (size_t)n_energies * n_timestep, 0.0);
   const Expansion ex_fwd = time_step_expansion(bes, n_bes);
-  // states per batch: the QE block (N x n_en x nb complex) must fit in memory
+  // states per batch: the QE block (N x n_en x nb complex) must fit in memory.
+  // When not even one state's block fits, the energies are taken in chunks:
+  // every chunk repeats the propagation of the batch for its own energies
+  // (the DOS correlation is taken from the first chunk only).
   int B = std::min(batch_size(c), kMaxCols / 2);
+  int en_chunk = std::max(n_en_inds, 1);
   {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && n_en_inds > 0) {
       // per state: its QE block (N x n_en complex) plus its two columns in
-      // the window ring (kMaxWindow + 1 slots) and in X, Y, wf0
+      // the window ring (kMaxWindow + 1 slots) and in X, Y, wf0; buffers this
+      // context already holds count as free
+      const size_t held = c->qe.bytes + c->A.bytes + c->X.bytes + c->Y.bytes + c->wf0.bytes;
+      const size_t avail = free_b + held;
       const size_t cx = 2 * real_size(c->ham.prec);
-      const size_t per_state =
-          (size_t)c->ham.n * ((size_t)n_en_inds * cx + (size_t)(kMaxWindow + 4) * 2 * cx);
+      const size_t ring = (size_t)c->ham.n * (size_t)(kMaxWindow + 4) * 2 * cx;
+      const size_t qe_1 = (size_t)c->ham.n * cx;  // one energy of one state
       const size_t reserve = (size_t)6 << 30;
-      const size_t budget = free_b > 2 * reserve ? free_b - reserve : free_b / 2;
-      const int fit = (int)std::max<size_t>(1, budget / std::max<size_t>(per_state, 1));
-      B = std::min(B, fit);
+      size_t budget = avail > 2 * reserve ? avail - reserve : avail / 2;
+      if (c->opts.dc_budget_gb > 0)
+        budget = std::min(budget, (size_t)(c->opts.dc_budget_gb * 1073741824.0));
+      const size_t per_state = (size_t)n_en_inds * qe_1 + ring;
+      const int fit = (int)std::min<size_t>((size_t)B, budget / std::max<size_t>(per_state, 1));
+      if (fit >= 1) {
+        B = fit;
+      } else {
+        B = 1;
+        en_chunk = budget > ring ? (int)std::min<size_t>((budget - ring) / qe_1, n_en_inds) : 0;
+        if (en_chunk < 1)
+          throw Error{TBPM_ERR_OOM,
+                      "tbpm_dccond: one state's propagation ring does not fit in device memory"};
+      }
     }
     (void)cudaGetLastError();
   }
@@ -1901,19 +1992,22 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
       kp = &keys;
     }
     const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
-    dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb, c->opts.vector_width), [&](auto tag) {
-      using P = decltype(tag);
-      dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep, t_step, en_sel,
-                                       chk_step, chk_thr, n_states, n_energies, dos_corr,
-                                       dc_corr);
-    });
+    for (int e0 = 0; e0 < std::max(n_en_inds, 1); e0 += en_chunk) {
+      const std::vector<double> part(
+          en_sel.begin() + std::min(e0, n_en_inds),
+          en_sel.begin() + std::min(e0 + en_chunk, n_en_inds));
+      dispatch(c->ham.prec, pick_V(c->ham.prec, 2 * nb, nb, c->opts.vector_width),
+               [&](auto tag) {
+                 using P = decltype(tag);
+                 dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep,
+                                                  t_step, part, chk_step, chk_thr, n_states,
+                                                  n_energies, dos_corr, dc_corr, nullptr,
+                                                  "tbpm_dccond", e0, e0 == 0);
+               });
+    }
   }
 }
 
-void release_blas(tbpm_ctx* c) {
-  if (c->blas && blas_api().ok) blas_api().destroy(reinterpret_cast<cublasHandle_t>(c->blas));
-  c->blas = nullptr;
-}
 
 void drv_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
                  const double* sx, const double* sy, const double* sz, const double* q_points,
@@ -2037,15 +2131,6 @@ void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
     throw Error{TBPM_ERR_ARG, "Error: wrong direction! (1: x, 2: y)"};
   if (!mu) throw Error{TBPM_ERR_ARG, "null output"};
   if (c->ham.n > (int64_t)INT32_MAX) throw Error{TBPM_ERR_ARG, "too many orbitals for the GEMM"};
-  const BlasApi& api = blas_api();
-  if (!api.ok) throw Error{TBPM_ERR_CUDA, "libcublas.so.12 could not be loaded"};
-  if (!c->blas) {
-    cublasHandle_t hnd = nullptr;
-    if (api.create(&hnd) != CUBLAS_STATUS_SUCCESS)
-      throw Error{TBPM_ERR_CUDA, "cublasCreate failed"};
-    c->blas = hnd;
-  }
-  api.set_stream(reinterpret_cast<cublasHandle_t>(c->blas), c->stream);
   c->launches = 0;
   c->model_bytes = 0;
   c->graph.reset();
@@ -2057,7 +2142,10 @@ void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
   c->A.ensure((size_t)n * n_kernel * cs);
   c->X.ensure((size_t)n * kc * cs);
   c->Y.ensure((size_t)n * 5 * cs);
-  c->qe.ensure((size_t)kc * n_kernel * cs);
+  {
+    const PqSplit sp = pq_split(c, n, kc, n_kernel);
+    c->qe.ensure((size_t)sp.slices * kc * n_kernel * sizeof(double2));
+  }
   // kpm.f90:8-29 Jackson kernel, first element halved
   std::vector<double> g(n_kernel);
   g[0] = 0.5;

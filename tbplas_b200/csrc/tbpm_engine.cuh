@@ -25,7 +25,8 @@ void throw_cuda(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) ::tbpm::throw_cuda(e_, #call); \
   } while (0)
 
-// Grow-only device allocation.
+// Grow-only device allocation, in multiples of 256 bytes (the bulk copies of
+// the ring kernels widen their windows to 16-byte boundaries and rely on it).
 struct DevMem {
   void* p = nullptr;
   size_t bytes = 0;
@@ -105,11 +106,11 @@ struct tbpm_ctx {
   tbpm::Ham ham;
   tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef, seg;
   tbpm::DevMem raw;  // device copy of an uploaded host CSR, kept for the next upload
+  tbpm::DevMem status;  // bit 0: a bounded device-side wait ran out (cleared when read)
   int64_t launches = 0;
   double model_bytes = 0;
   tbpm::Session sess;
   tbpm::GraphCache graph;
-  void* blas = nullptr;  // cublasHandle_t of the Kubo-Bastin GEMMs (created on first use)
   // device address of the allocation-free time step's fixed work array on this
   // context's device (tbpm_noalloc.cu), looked up on its first call
   void* noalloc_scratch = nullptr;

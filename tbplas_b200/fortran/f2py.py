@@ -36,6 +36,8 @@ _backend = {
     "use_graphs": True,
     "fp32_chk_thr": 1.0e-4,
     "vector_width": 0,       # complex values per thread: 0 auto (32-byte accesses), 1, 2
+    "term_kernel": 0,        # Chebyshev-term kernel: 0 auto (shared-memory ring), 1 grid-stride
+    "dc_budget_gb": 0.0,     # DC quasi-eigenstate memory budget in GiB (0: free memory)
     "verbose": False,
 }
 
@@ -69,6 +71,8 @@ def _ctx() -> nat.Context:
         use_graphs=1 if _backend["use_graphs"] else 0,
         fp32_chk_thr=float(_backend["fp32_chk_thr"]),
         vector_width=int(_backend["vector_width"]),
+        term_kernel=int(_backend["term_kernel"]),
+        dc_budget_gb=float(_backend["dc_budget_gb"]),
     )
     return ctx
 

@@ -109,3 +109,24 @@ def test_dc_fp32_error_bound(sample):
     print(f"FP32 DC relative error: dos {e_dos:.2e}, dc {e_dc:.2e}")
     assert e_dos < FP32_TOL
     assert e_dc < FP32_TOL
+
+
+@pytest.mark.parametrize("budget_kb", [70, 150])
+def test_dc_within_a_memory_budget_matches_oracle(sample, budget_kb):
+    """A memory budget smaller than the quasi-eigenstate block of all states
+    (96 orbitals, 17 energies: 1.5 KB per energy and state, 60 KB of state
+    ring per state).  150 KB holds one state's block, so the states run one
+    per batch; 70 KB does not, so the energies are taken in chunks of six,
+    each chunk repeating the propagation.  Results equal the unconstrained
+    run's to rounding and the oracle's to the FP64 bar."""
+    f2py.set_backend(batch=3)
+    free, _, sel = _run(sample, 3, 40, (-2.0, 2.0), seed=5)
+    assert sel.size == 17
+    f2py.set_backend(dc_budget_gb=budget_kb / 2**20)
+    try:
+        got, ref, _ = _run(sample, 3, 40, (-2.0, 2.0), seed=5)
+    finally:
+        f2py.set_backend(dc_budget_gb=0.0)
+    for k in (0, 1):
+        assert rel_err(got[k], free[k]) < 1e-13
+        assert rel_err(got[k], ref[k]) < FP64_TOL

@@ -166,3 +166,53 @@ def test_cheb_timestep_multi_sweep(g256):
     back = np.stack([oracle.cheb_timestep(bes, h.indptr, h.indices, h.data, ref[b],
                                           forward=False) for b in range(16)])
     assert rel_err(got, back) < 1e-12
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_ring_and_grid_stride_term_kernels_agree(g256, prec):
+    """The shared-memory ring kernel computes every element in the order of the
+    grid-stride kernel: time-stepped states are bit-identical, correlations
+    (whose block partials group differently) agree to rounding."""
+    h = g256.build_ham_csr()
+    n = h.shape[0]
+    wf0 = unit_states(16, n, seed=19)
+    bes = bessel_series(math.pi)
+    out = {}
+    for kernel in (1, 2):
+        f2py.set_backend(precision=prec, term_kernel=kernel)
+        out[kernel] = (f2py.tbpm_dos_states(bes, h.indptr, h.indices, h.data, wf0, 8, 4, 1e-9),
+                       f2py.tbpm_psi_t(bes, h.indptr, h.indices, h.data, wf0[3],
+                                       np.array([0, 5]), 5, 4, 1e-9))
+    f2py.set_backend(term_kernel=0)
+    assert np.array_equal(out[1][1], out[2][1])
+    assert rel_err(out[2][0], out[1][0]) < (1e-13 if prec == "fp64" else 1e-6)
+
+
+def test_ring_kernel_with_a_dense_row(graphene_small):
+    """One row coupled to 300 others: its tile holds more CSR entries than a
+    ring stage, so that tile's entries are read from global memory."""
+    h = graphene_small.build_ham_csr()
+    n = h.shape[0]
+    rows, cols, vals = [], [], []
+    for r in range(n):
+        a, b = h.indptr[r], h.indptr[r + 1]
+        c, v = list(h.indices[a:b]), list(h.data[a:b])
+        if r == 5:
+            c += list(range(60, 360))
+            v += [0.001 * (1 + 0.5j)] * 300
+        elif 60 <= r < 360:
+            c += [5]
+            v += [0.001 * (1 - 0.5j)]
+        order = np.argsort(c)
+        rows += [r] * len(c)
+        cols += list(np.asarray(c)[order])
+        vals += list(np.asarray(v)[order])
+    ip = np.zeros(n + 1, dtype=np.int32)
+    np.cumsum(np.bincount(rows, minlength=n), out=ip[1:])
+    ix = np.array(cols, dtype=np.int32)
+    hv = np.array(vals, dtype=np.complex128)
+    wf0 = unit_states(16, n, seed=8)
+    bes = bessel_series(math.pi)
+    got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 12, 128, 1e-9)
+    ref = oracle.tbpm_dos(bes, ip, ix, hv, 12, wf0=wf0)
+    assert rel_err(got, ref) < FP64_TOL
