@@ -224,6 +224,22 @@ int tbpm_dccond_states(tbpm_ctx* ctx, const double* bes, int n_bes, const int32_
                        int n_en_inds, int wfn_chk_step, double wfn_chk_thr,
                        double* dos_corr, double* dc_corr);
 
+/* Part of a tbpm_dccond run on the resident Hamiltonian (uploaded with dx, dy):
+ * the states [first_state, first_state + n_states) of a run of n_ran_samples
+ * states.  Their contributions, each divided by n_ran_samples, are ADDED to
+ * dos_corr and dc_corr (layouts as tbpm_dccond) in the order tbpm_dccond adds
+ * them, so a run taken in consecutive parts with the outputs kept in between
+ * reproduces the same sums; DC checkpointing saves the outputs between parts.
+ * States are seeded as in tbpm_dccond (seed, rank, n_ran_samples), or, if wf0
+ * is not NULL, wf0 = complex128 [n_states][n_rows] holds this part's states.
+ * No counterpart in the reference (its run is one call). */
+int tbpm_dccond_accumulate(tbpm_ctx* ctx, const double* bes, int n_bes, const double* wf0,
+                           int seed, int rank, int n_ran_samples, int first_state, int n_states,
+                           int n_timestep, double t_step, const double* energies,
+                           int n_energies, const int32_t* en_inds, int n_en_inds,
+                           int wfn_chk_step, double wfn_chk_thr, double* dos_corr,
+                           double* dc_corr);
+
 /* tbpm_psi_t -- replaces tbpm.f90:1029-1093 (SUBROUTINE tbpm_psi_t) as called
  * from Solver.calc_psi_t (tbpm/solver.py:543-600).
  * psi0: complex128[n_rows]; time_log: int32[n_time_log] sorted, unique, in
@@ -377,6 +393,38 @@ int tbpm_cheb_timestep_noalloc(tbpm_ctx* ctx, const double* bes, int n_bes,
                                const int32_t* indptr, const int32_t* indices,
                                const double* hop, int64_t n_rows, int64_t nnz, double* wf,
                                int n_states, int forward);
+
+/* Self-test of the device-side failure path (no counterpart in the reference,
+ * whose only failure check is check_norm): one block waits, with the bounded
+ * wait of the Chebyshev-term ring kernels, on a shared-memory barrier that
+ * nothing completes.  The wait gives up after 2 s and records it in the
+ * context's status word; the call then returns TBPM_ERR_TIMEOUT, as a
+ * propagation whose wait ran out would, and the context stays usable. */
+int tbpm_selftest_wait_timeout(tbpm_ctx* ctx);
+
+/* ---- Analyzer transforms on the device ---------------------------------- */
+
+/* Window-weighted trigonometric sums of correlation functions, the
+ * O(tnr^2) part of Analyzer.calc_ac_cond (analysis.py:161-243) and
+ * calc_dyn_pol (:245-308) and the sums of calc_dc_cond (:375-458).  For output
+ * o = r * n_x + i:
+ *   out_cos[o] = sum_k w[k] a[q][k] cos(phase_ik),
+ *   out_sin[o] = sum_k w[k] b[q][k] sin(phase_ik),
+ * k < n_k, with phase_ik = (x[i] * k) * dt, or x[i] * (k * dt) when phase_kdt is
+ * 1, and q = r (per_output = 0: a, b are [n_rows][n_k]) or q = o (per_output =
+ * 1: a, b are [n_rows][n_x][n_k]).  Either output may be NULL (its coefficient
+ * array is then not read).  Host arrays; synchronous. */
+int tbpm_trig_sums(tbpm_ctx* ctx, const double* w, int n_k, const double* a, const double* b,
+                   int n_rows, const double* x, int n_x, double dt, int per_output,
+                   int phase_kdt, double* out_cos, double* out_sin);
+/* The cumulative trapezoid of Analyzer.calc_diff_coeff (analysis.py:460-511):
+ * for row q < n_rows, y_k = (a[q][k] cos(x[q] k dt) + b[q][k] sin(x[q] k dt)) w[k]
+ * and out[q][0] = 0, out[q][j] = out[q][j-1] + (spacing[j-1] (y_{j-1} + y_j)) / 2
+ * (scipy's cumulative_trapezoid over a grid with the given spacing).  Host
+ * arrays; synchronous. */
+int tbpm_trig_cumtrapz(tbpm_ctx* ctx, const double* w, int n_k, const double* a,
+                       const double* b, int n_rows, const double* x, double dt,
+                       const double* spacing, double* out);
 
 /* ---- learned C(t) tail extrapolator: BF16 kernels, FP32 accumulation ------
  * No counterpart in the reference (TBPLaS has no learned component).  All

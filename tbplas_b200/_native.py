@@ -46,7 +46,8 @@ EXPORTED_SYMBOLS = (
     "tbpm_supercell_csr", "tbpm_dyn_pol", "tbpm_dyn_pol_states", "tbpm_eigenstates",
     "tbpm_eigenstates_states", "tbpm_kbdc", "tbpm_kbdc_states", "tbpm_haydock_coef",
     "tbpm_cond_from_trace", "tbpm_session_export", "tbpm_session_dos_resume",
-    "tbpm_nn_gemm_tn_mma", "tbpm_nn_tc_status",
+    "tbpm_nn_gemm_tn_mma", "tbpm_nn_tc_status", "tbpm_trig_sums", "tbpm_trig_cumtrapz",
+    "tbpm_selftest_wait_timeout", "tbpm_dccond_accumulate",
 )
 
 
@@ -60,6 +61,11 @@ class TbpmError(RuntimeError):
 
 class NormError(TbpmError):
     """Wave-function norm check failed (the reference Fortran `stop`s here)."""
+
+
+class DeviceTimeoutError(TbpmError):
+    """A bounded device-side wait ran out (TBPM_ERR_TIMEOUT); the results of
+    that call are invalid, the context stays usable."""
 
 
 class NanError(NormError):
@@ -201,6 +207,14 @@ _SIGNATURES = {
     "tbpm_supercell_csr": (_c_int, [_vp, ctypes.POINTER(Supercell), _c_int, _c_dbl,
                                     ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64),
                                     ctypes.POINTER(_c_dbl), _vp, _vp, _vp, _vp, _vp]),
+    "tbpm_selftest_wait_timeout": (_c_int, [_vp]),
+    "tbpm_dccond_accumulate": (_c_int, [_vp, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
+                                        _c_int, _c_int, _c_dbl, _vp, _c_int, _vp, _c_int,
+                                        _c_int, _c_dbl, _vp, _vp]),
+    "tbpm_trig_sums": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_dbl,
+                                _c_int, _c_int, _vp, _vp]),
+    "tbpm_trig_cumtrapz": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_dbl, _vp,
+                                    _vp]),
 }
 
 _lib = None
@@ -247,6 +261,8 @@ def raise_for(code: int, message: str) -> None:
         raise NanError(code, message)
     if code == TBPM_ERR_OOM:
         raise MemoryError(message)
+    if code == TBPM_ERR_TIMEOUT:
+        raise DeviceTimeoutError(code, message)
     raise TbpmError(code, message)
 
 

@@ -1,4 +1,4 @@
-"""Checkpoint and resume of long DOS propagations.
+"""Checkpoint and resume of long DOS and DC propagations.
 
 The reference's TBPM drivers hold their state inside one Fortran call
 (tbplas/fortran/tbpm.f90:6-93), so a run that is interrupted starts again from
@@ -17,6 +17,10 @@ Called again with the same inputs and path, it resumes from that file
 (tbpm_session_dos_resume) and returns exactly what an uninterrupted run
 returns.  A file whose fingerprint does not match is ignored.  The file is
 written atomically (temporary file + rename) and removed when the run ends.
+
+`dc_checkpointed` does the same for f2py.tbpm_dccond (tbpm.f90:497-718) at the
+boundaries between parts of the state list (the per-batch quasi-eigenstate
+block is too large to write out mid-batch).
 """
 
 import ctypes
@@ -30,7 +34,7 @@ import numpy as np
 from . import _native as nat
 from .fortran import f2py
 
-__all__ = ["dos_checkpointed", "fingerprint"]
+__all__ = ["dos_checkpointed", "dc_checkpointed", "fingerprint"]
 
 
 def _crc(a: np.ndarray) -> int:
@@ -177,3 +181,74 @@ def dos_checkpointed(bes, s_indptr, s_indices, s_hop, seed, n_timestep, n_ran_sa
     if os.path.exists(path):
         os.remove(path)
     return corr
+
+
+def dc_checkpointed(bes, s_indptr, s_indices, s_hop, h_rescale, s_dx, s_dy, seed, n_timestep,
+                    n_ran_samples, t_step, energies, en_inds, rank, wfn_chk_step, wfn_chk_thr,
+                    path: str, states_per_part: Optional[int] = None,
+                    on_checkpoint: Optional[Callable[[int], None]] = None):
+    """f2py.tbpm_dccond (tbpm.f90:497-718) with a checkpoint file at `path`.
+
+    A DC run keeps, per batch of states, the quasi-eigenstate block (N x
+    energies x states complex values, tens of GB at the largest samples) on
+    the device, so it is checkpointed between parts of the state list: the
+    run is taken in parts of `states_per_part` states (default: the backend's
+    batch width), each added to the DOS and DC correlations by
+    tbpm_dccond_accumulate, and after every part the two arrays and the
+    number of finished states are written atomically with a fingerprint of
+    every input.  A later call with the same inputs continues after the last
+    finished part and returns what an uninterrupted call with the same parts
+    returns, bit for bit.
+
+    :param on_checkpoint: called as on_checkpoint(states_done) after each write
+    :return: (dos_corr (n_timestep,), dc_corr (2, len(energies), n_timestep) F-order)
+    """
+    be = f2py.get_backend()
+    bes = nat.as_c(bes, np.float64)
+    en = nat.as_c(energies, np.float64)
+    ei = nat.as_c(en_inds, np.int32)
+    tnr, n_avg = int(n_timestep), int(n_ran_samples)
+    if tnr < 1 or n_avg < 1:
+        raise ValueError("n_timestep and n_ran_samples must be >= 1")
+    part = int(states_per_part) if states_per_part else max(1, min(int(be["batch"]), 32))
+    if part < 1:
+        raise ValueError("states_per_part must be >= 1")
+    ctx = f2py._ctx()
+    if hasattr(s_indptr, "make_resident"):
+        s_indptr.make_resident(ctx)
+    else:
+        ip, ix, hv, n, nnz = f2py._csr(s_indptr, s_indices, s_hop)
+        dx, dy = f2py._real(s_dx, nnz), f2py._real(s_dy, nnz)
+        ctx.call("tbpm_ham_upload", nat.ptr(ip), nat.ptr(ix), nat.ptr(hv), n, nnz, nat.ptr(dx),
+                 nat.ptr(dy), float(h_rescale))
+    h = hashlib.sha256()
+    h.update(fingerprint(bes, s_indptr, s_indices, s_hop, seed, tnr, n_avg, rank, be).encode())
+    if not hasattr(s_indptr, "make_resident"):
+        for a in (s_dx, s_dy):
+            h.update(str(_crc(np.ascontiguousarray(a, dtype=np.float64))).encode())
+    h.update(repr((float(h_rescale), float(t_step), part, int(wfn_chk_step),
+                   float(wfn_chk_thr))).encode())
+    h.update(en.tobytes())
+    h.update(ei.tobytes())
+    fp = h.hexdigest()
+    state = _load(path, fp)
+    dos = np.zeros(tnr, dtype=np.complex128)
+    dc = np.zeros((2, en.size, tnr), dtype=np.complex128, order="F")
+    s0 = 0
+    if state is not None:
+        dos = np.ascontiguousarray(state["dos"])
+        dc = np.asfortranarray(state["dc"])
+        s0 = int(state["s0"])
+    while s0 < n_avg:
+        k = min(part, n_avg - s0)
+        ctx.call("tbpm_dccond_accumulate", nat.ptr(bes), bes.size, None, int(seed), int(rank),
+                 n_avg, s0, k, tnr, float(t_step), nat.ptr(en), en.size, nat.ptr(ei), ei.size,
+                 int(wfn_chk_step), float(wfn_chk_thr), nat.ptr(dos), nat.ptr(dc))
+        s0 += k
+        if s0 < n_avg:
+            _save(path, fingerprint=np.array(fp), s0=np.array(s0), dos=dos, dc=dc)
+            if on_checkpoint is not None:
+                on_checkpoint(s0)
+    if os.path.exists(path):
+        os.remove(path)
+    return dos, dc

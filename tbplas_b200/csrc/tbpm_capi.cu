@@ -20,6 +20,11 @@ void drv_ac(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
             const double* wf0, int n_states, int seed, int rank, int n_ran_samples,
             int n_timestep, int nr_fermi, double fermi_precision, int chk_step, double chk_thr,
             double* corr);
+void drv_dc_part(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int first_state,
+                 int n_states, int n_avg, int seed, int rank, int n_ran_samples, int n_timestep,
+                 double t_step, const double* energies, int n_energies, const int32_t* en_inds,
+                 int n_en_inds, int chk_step, double chk_thr, double* dos_corr, double* dc_corr,
+                 bool zero);
 void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
             int seed, int rank, int n_ran_samples, int n_timestep, double t_step,
             const double* energies, int n_energies, const int32_t* en_inds, int n_en_inds,
@@ -39,6 +44,7 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
                        double chk_thr, double* corr, double* corr_per_state);
 void drv_session_advance(tbpm_ctx* c, int n_steps);
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done);
+void drv_selftest_wait_timeout(tbpm_ctx* c);
 void drv_session_dos_resume(tbpm_ctx* c, const double* bes, int n_bes, int n_states,
                             const double* wf0, const double* psi, const double* corr,
                             const double* norms, int n_done, int n_timestep);
@@ -437,6 +443,21 @@ int tbpm_dccond_states(tbpm_ctx* c, const double* bes, int n_bes, const int32_t*
   });
 }
 
+int tbpm_dccond_accumulate(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0,
+                           int seed, int rank, int n_ran_samples, int first_state, int n_states,
+                           int n_timestep, double t_step, const double* energies,
+                           int n_energies, const int32_t* en_inds, int n_en_inds,
+                           int wfn_chk_step, double wfn_chk_thr, double* dos_corr,
+                           double* dc_corr) {
+  return guarded(c, [&] {
+    if (n_states < 1 || first_state < 0 || first_state + n_states > n_ran_samples)
+      throw tbpm::Error{TBPM_ERR_ARG, "states outside [0, n_ran_samples)"};
+    tbpm::drv_dc_part(c, bes, n_bes, wf0, first_state, n_states, n_ran_samples, seed, rank,
+                      n_ran_samples, n_timestep, t_step, energies, n_energies, en_inds,
+                      n_en_inds, wfn_chk_step, wfn_chk_thr, dos_corr, dc_corr, false);
+  });
+}
+
 int tbpm_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const int32_t* indptr,
                const int32_t* indices, const double* hop, int64_t n_rows, int64_t nnz,
                const double* psi0, const int32_t* time_log, int n_time_log, int n_timestep,
@@ -514,6 +535,10 @@ int tbpm_session_advance(tbpm_ctx* c, int n_steps) {
 
 int tbpm_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done) {
   return guarded(c, [&] { tbpm::drv_session_read(c, corr, norms, n_done); });
+}
+
+int tbpm_selftest_wait_timeout(tbpm_ctx* c) {
+  return guarded(c, [&] { tbpm::drv_selftest_wait_timeout(c); });
 }
 
 int tbpm_session_export(tbpm_ctx* c, double* wf0, double* psi) {

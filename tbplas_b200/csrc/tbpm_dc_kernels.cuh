@@ -215,6 +215,159 @@ __global__ void __launch_bounds__(256, TBPM_QE_MINB_A) qe_accum_kernel(
   }
 }
 
+// ---- quasi-eigenstate accumulation as FP64 matrix products (mma.sync) -------
+//
+// For a row r and state b the window update of qe_accum_kernel is, over the
+// energies i,
+//   QE_re[i] += sum_tau Re c[tau][i] S_tau.x - Im c[tau][i] D_tau.y
+//   QE_im[i] += sum_tau Re c[tau][i] S_tau.y + Im c[tau][i] D_tau.x
+// i.e. one real product  A (energies x 2T) . B (2T x (r, b, re/im))  added to
+// the block QE, with A[i][tau] = Re c, A[i][16 + tau] = Im c (zero for tau >=
+// T) shared by every row.  qe_accum_mma_kernel runs it on the FP64 tensor
+// path (mma.sync m8n8k4 f64): a warp owns up to kQeMmaMT tiles of 8 energies
+// and keeps their A fragments (8 k-steps of 4) in registers for the whole
+// launch; for each tile of kQeMmaPairs (row, state) pairs the block stages S
+// and D (double) in shared memory, and a warp then, per 8-column tile (4 pairs
+// x re/im), loads the B fragments once and updates its energy tiles: the C
+// fragment of a lane is exactly one complex QE element.  QE is read and
+// written once per window.
+constexpr int kQeMmaWarps = 8;
+constexpr int kQeMmaMT = 4;      // energy tiles (of 8) per warp
+constexpr int kQeMmaPairs = 32;  // (row, state) pairs per staged tile
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Rows per staged tile: at least kQeMmaPairs pairs, and rows * nb a multiple
+// of 4 (whole 8-column tiles).
+__host__ __device__ constexpr int qe_mma_rows(int nb) {
+  return (((kQeMmaPairs + nb - 1) / nb) + (4 / (nb % 4 == 0 ? 4 : (nb % 2 == 0 ? 2 : 1))) - 1) /
+         (4 / (nb % 4 == 0 ? 4 : (nb % 2 == 0 ? 2 : 1))) *
+         (4 / (nb % 4 == 0 ? 4 : (nb % 2 == 0 ? 2 : 1)));
+}
+
+// Shared memory of qe_accum_mma_kernel: S and D of a tile, [tau][pair].
+__host__ __device__ constexpr size_t qe_mma_smem(int nb) {
+  return (size_t)kMaxWindow * qe_mma_rows(nb) * nb * 2 * sizeof(double2);
+}
+
+// Grid: x walks tiles of qe_mma_rows(nb) rows grid-stride; y walks groups of
+// kQeMmaWarps * kQeMmaMT energy tiles.  Block: kQeMmaWarps warps.
+template <typename R>
+__global__ void __launch_bounds__(kQeMmaWarps * 32, 2) qe_accum_mma_kernel(
+    typename Cx<R>::t* qe, int64_t n_rows, int n_en, int nb, const __grid_constant__ StatePtrs<R> win, int T,
+    const double2* coef, int init, const typename Cx<R>::t* wf0) {
+  using C = typename Cx<R>::t;
+  extern __shared__ double2 qsm[];
+  const int RT = qe_mma_rows(nb);
+  const int P = RT * nb;  // pairs of a tile; P % 4 == 0
+  const int ld = 2 * nb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // The block's energy tiles [blockIdx.y * 32, +32) form n_mg groups of
+  // kQeMmaMT; warp w takes group w % n_mg and, with the other warps of that
+  // group, every cnt-th column tile (so few energies still use every warp).
+  const int n_mt = (n_en + 7) / 8;
+  const int mt_b = blockIdx.y * kQeMmaWarps * kQeMmaMT;
+  const int n_mt_b = min(kQeMmaWarps * kQeMmaMT, n_mt - mt_b);
+  const int n_mg = (n_mt_b + kQeMmaMT - 1) / kQeMmaMT;
+  const int mg = warp % n_mg;
+  const int nt_first = warp / n_mg;
+  const int nt_step = (kQeMmaWarps - mg + n_mg - 1) / n_mg;
+  const int mt0 = mt_b + mg * kQeMmaMT;
+  // A fragments: A[i = 8*mt + g][k = 4*s + t]
+  double afr[kQeMmaMT][8];
+#pragma unroll
+  for (int m = 0; m < kQeMmaMT; ++m) {
+    const int i = (mt0 + m) * 8 + g;
+#pragma unroll
+    for (int st = 0; st < 8; ++st) {
+      const int k = 4 * st + t;
+      const int tau = k & 15;
+      double v = 0.0;
+      if (i < n_en && tau < T) {
+        const double2 c = coef[tau * n_en + i];
+        v = k < 16 ? c.x : c.y;
+      }
+      afr[m][st] = v;
+    }
+  }
+  double2* sS = qsm;                          // [kMaxWindow][P]
+  double2* sD = qsm + kMaxWindow * P;         // [kMaxWindow][P]
+  for (int64_t r0 = (int64_t)blockIdx.x * RT; r0 < n_rows; r0 += (int64_t)gridDim.x * RT) {
+    const int nr = (int)min((int64_t)RT, n_rows - r0);
+    __syncthreads();  // the previous tile's S / D are consumed
+    for (int q = threadIdx.x; q < kMaxWindow * P; q += blockDim.x) {
+      const int tau = q / P;
+      const int pr = q - tau * P;
+      const int rr = pr / nb, bb = pr - rr * nb;
+      double2 S = make_double2(0.0, 0.0), D = make_double2(0.0, 0.0);
+      if (tau < T && rr < nr) {
+        const C* src = win.p[tau] + (r0 + rr) * ld;
+        const C pv = ldg_c(src + bb);
+        const C mv = ldg_c(src + nb + bb);
+        S = make_double2((double)pv.x + (double)mv.x, (double)pv.y + (double)mv.y);
+        D = make_double2((double)pv.x - (double)mv.x, (double)pv.y - (double)mv.y);
+      }
+      sS[q] = S;
+      sD[q] = D;
+    }
+    __syncthreads();
+    for (int nt = nt_first; nt < P / 4; nt += nt_step) {
+      // B fragment: B[k = 4*s + t][n = g]; column g is pair 4*nt + g/2, part g&1
+      const int pb = 4 * nt + (g >> 1);
+      const bool im = g & 1;
+      double bfr[8];
+#pragma unroll
+      for (int st = 0; st < 8; ++st) {
+        const int k = 4 * st + t;
+        if (k < 16) {
+          const double2 S = sS[k * P + pb];
+          bfr[st] = im ? S.y : S.x;
+        } else {
+          const double2 D = sD[(k - 16) * P + pb];
+          bfr[st] = im ? D.x : -D.y;
+        }
+      }
+      // C fragment: energy 8*mt + g, pair 4*nt + t (re, im)
+      const int pc = 4 * nt + t;
+      const int rr = pc / nb, bb = pc - rr * nb;
+      const bool row_ok = rr < nr;
+      double c0[kQeMmaMT], c1[kQeMmaMT];
+#pragma unroll
+      for (int m = 0; m < kQeMmaMT; ++m) {
+        const int i = (mt0 + m) * 8 + g;
+        c0[m] = c1[m] = 0.0;
+        if (row_ok && i < n_en) {
+          const C v = init ? wf0[(r0 + rr) * nb + bb] : qe[((r0 + rr) * n_en + i) * nb + bb];
+          c0[m] = (double)v.x;
+          c1[m] = (double)v.y;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < kQeMmaMT; ++m) {
+        if (mt0 + m < n_mt) {
+#pragma unroll
+          for (int st = 0; st < 8; ++st) dmma_8x8x4(c0[m], c1[m], afr[m][st], bfr[st]);
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < kQeMmaMT; ++m) {
+        const int i = (mt0 + m) * 8 + g;
+        if (row_ok && i < n_en) {
+          C o;
+          o.x = (R)c0[m];
+          o.y = (R)c1[m];
+          qe[((r0 + rr) * n_en + i) * nb + bb] = o;
+        }
+      }
+    }
+  }
+}
+
 // Tall-skinny reductions over orbitals: block partial sums of
 // conj(u_tau[r][k*nb + b]) * QE[r][i][b] for tau < T, k in {0, 1} (mode 0), or
 // of conj(wf0[r][b]) * QE[r][i][b] (mode 1, T = 1, k = 0).
@@ -356,6 +509,107 @@ __global__ void __launch_bounds__(256, TBPM_QE_MINB_P) qe_project_kernel(
         partials[(o * 2 + 1) * gridDim.x + blockIdx.x] = ai[tau][g];
       }
     }
+  }
+}
+
+// ---- quasi-eigenstate projections as FP64 matrix products (mma.sync) -------
+//
+// For a state b, the projections of qe_project_kernel over the rows r of a
+// block's range are a real product  A (32 x 2R) . B (2R x energies):  row
+// mm = 2m + c of A (m = tau*K + k, c = re/im of the result) and column
+// (r, part) of B = Re / Im QE[r][i][b]:
+//   A[2m][(r,0)] =  Re u,  A[2m][(r,1)] = Im u,
+//   A[2m+1][(r,0)] = -Im u, A[2m+1][(r,1)] = Re u,   u = u_tau[r][k*nb + b]
+// (wf0[r][b] in mode 1), which gives sum_r conj(u) QE.  A warp owns one state
+// b and kQeProjNT tiles of 8 energies, and walks its block's rows two at a
+// time (one k-step of mma.sync m8n8k4 f64): 4 A fragments (from u, shared by
+// its energy tiles) and one B fragment per energy tile (QE) per step.  The
+// block partials have the layout of qe_project_kernel.
+constexpr int kQeProjNT = 4;
+
+template <typename R>
+__global__ void __launch_bounds__(kQeMmaWarps * 32, 2) qe_project_mma_kernel(
+    const typename Cx<R>::t* qe, int64_t n_rows, int64_t rows_per_tile, int n_en, int nb,
+    const __grid_constant__ StatePtrs<R> u, int T, int mode, const typename Cx<R>::t* wf0,
+    double* partials) {
+  using C = typename Cx<R>::t;
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
+  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
+  const int n_ib = n_en * nb;
+  const int K = mode == 0 ? 2 : 1;
+  const int M = mode == 0 ? T * K : 1;  // complex results per element
+  const int ld = 2 * nb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int n_nt = (n_en + 7) / 8;
+  const int groups = (n_nt + kQeProjNT - 1) / kQeProjNT;
+  const int task = blockIdx.y * kQeMmaWarps + warp;  // (state, group of energy tiles)
+  if (task >= nb * groups) return;
+  const int b = task % nb;
+  const int nt0 = (task / nb) * kQeProjNT;
+  double acc[4][kQeProjNT][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int j = 0; j < kQeProjNT; ++j) acc[mt][j][0] = acc[mt][j][1] = 0.0;
+  for (int64_t rp = r0; rp < r1; rp += 2) {
+    // k index 4*0 + t: row rp + t/2, part t&1
+    const int64_t r = rp + (t >> 1);
+    const bool rok = r < r1;
+    const int part = t & 1;
+    double afr[4];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      const int mm = 8 * mt + g;
+      const int m = mm >> 1, c = mm & 1;
+      double v = 0.0;
+      if (rok && m < M) {
+        C w;
+        if (mode == 0) {
+          const int tau = m / K, k = m - tau * K;
+          w = u.p[tau][r * ld + k * nb + b];
+        } else {
+          w = wf0[r * nb + b];
+        }
+        const double ur = (double)w.x, ui = (double)w.y;
+        v = c == 0 ? (part == 0 ? ur : ui) : (part == 0 ? -ui : ur);
+      }
+      afr[mt] = v;
+    }
+    double bfr[kQeProjNT];
+#pragma unroll
+    for (int j = 0; j < kQeProjNT; ++j) {
+      const int i = (nt0 + j) * 8 + g;
+      double v = 0.0;
+      if (rok && i < n_en) {
+        const C q = qe[(r * n_en + i) * nb + b];
+        v = part == 0 ? (double)q.x : (double)q.y;
+      }
+      bfr[j] = v;
+    }
+#pragma unroll
+    for (int j = 0; j < kQeProjNT; ++j)
+      if (nt0 + j < n_nt) {
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) dmma_8x8x4(acc[mt][j][0], acc[mt][j][1], afr[mt], bfr[j]);
+      }
+  }
+  // C[mm][n]: lane holds rows mm = 8*mt + g, columns n = 2t, 2t+1 (energies)
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int mm = 8 * mt + g;
+    const int m = mm >> 1, c = mm & 1;
+    if (m >= M) continue;
+#pragma unroll
+    for (int j = 0; j < kQeProjNT; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int i = (nt0 + j) * 8 + 2 * t + q;
+        if (nt0 + j < n_nt && i < n_en) {
+          const int64_t o = (int64_t)m * n_ib + (int64_t)i * nb + b;
+          partials[(o * 2 + c) * gridDim.x + blockIdx.x] = acc[mt][j][q];
+        }
+      }
   }
 }
 

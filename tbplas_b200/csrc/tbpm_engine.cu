@@ -292,8 +292,9 @@ RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode) {
   s.hop_off = off;
   off += al((size_t)cap * cs);
   s.stage_bytes = off;
-  // two resident blocks per SM (228 KB of shared memory, 1 KB reserved per block)
-  const int budget = (228 * 1024) / 2 - 1024 - 256;
+  // kRingMinBlocks resident blocks per SM (228 KB of shared memory, 1 KB
+  // reserved per block)
+  const int budget = (228 * 1024) / kRingMinBlocks - 1024 - 256;
   const int S = std::min(kRingMaxStages, budget / off);
   if (S < 2) return RingShape{};
   s.rows = TR;
@@ -1071,6 +1072,9 @@ void ac_batch(tbpm_ctx* c, const Expansion& ex_time, const Expansion& ex_fermi, 
 // The QE kernels may need more than the default 48 KB of dynamic shared
 // memory (row tiles).  The attribute belongs to the current device, so it is
 // set before every launch that needs it (a host-side call, once per window).
+#ifndef TBPM_QE_MMA
+#define TBPM_QE_MMA 1  // quasi-eigenstate accumulation on mma.sync f64 (0: FMA kernel)
+#endif
 template <class K>
 void qe_smem_attr(K kernel, size_t bytes) {
   if (bytes <= 48 * 1024) return;
@@ -1162,16 +1166,30 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       StatePtrs<R> win{};
       for (int tau = 0; tau < len; ++tau) win.p[tau] = reinterpret_cast<const C*>(slot(tau));
       const int64_t total = n * n_en * nb;
-      const int qthreads = qe_accum_threads(n_en, nb);
-      const int n_chunks = (n_en * nb + kQeG * qthreads - 1) / (kQeG * qthreads);
-      const int64_t tiles = (n + qe_accum_rows<R>(nb) - 1) / qe_accum_rows<R>(nb);
-      const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)kSMs * 16), (unsigned)n_chunks);
-      const size_t qsmem = qe_accum_smem<R>(n_en, nb);
-      qe_accum_attr<R>(qsmem);
-      qe_accum_kernel<R><<<grid, qthreads, qsmem, c->stream>>>(qe, n, n_en, nb, win, len,
-                                                        c->coef.as<double2>(),
-                                                        first_window ? 1 : 0,
-                                                        reinterpret_cast<const C*>(W));
+      if (TBPM_QE_MMA) {
+        // FP64 tensor-path products (qe_accum_mma_kernel)
+        const int rt = qe_mma_rows(nb);
+        const int64_t tiles = (n + rt - 1) / rt;
+        const int groups = ((n_en + 7) / 8 + kQeMmaWarps * kQeMmaMT - 1) / (kQeMmaWarps * kQeMmaMT);
+        const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)num_sms(c->device) * 4),
+                        (unsigned)groups);
+        const size_t qsmem = qe_mma_smem(nb);
+        qe_smem_attr(qe_accum_mma_kernel<R>, qsmem);
+        qe_accum_mma_kernel<R><<<grid, kQeMmaWarps * 32, qsmem, c->stream>>>(
+            qe, n, n_en, nb, win, len, c->coef.as<double2>(), first_window ? 1 : 0,
+            reinterpret_cast<const C*>(W));
+      } else {
+        const int qthreads = qe_accum_threads(n_en, nb);
+        const int n_chunks = (n_en * nb + kQeG * qthreads - 1) / (kQeG * qthreads);
+        const int64_t tiles = (n + qe_accum_rows<R>(nb) - 1) / qe_accum_rows<R>(nb);
+        const dim3 grid((unsigned)std::min<int64_t>(tiles, (int64_t)kSMs * 16),
+                        (unsigned)n_chunks);
+        const size_t qsmem = qe_accum_smem<R>(n_en, nb);
+        qe_accum_attr<R>(qsmem);
+        qe_accum_kernel<R><<<grid, qthreads, qsmem, c->stream>>>(
+            qe, n, n_en, nb, win, len, c->coef.as<double2>(), first_window ? 1 : 0,
+            reinterpret_cast<const C*>(W));
+      }
       TBPM_CK(cudaGetLastError());
       c->launches++;
       c->model_bytes += (double)total * 2 * sizeof(R) * (first_window ? 1 : 2) +
@@ -1242,10 +1260,19 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   // |<wf0|QE_i>| per (energy, state)
   ensure_partials(c, (size_t)2 * n_ib * pgrid);
   c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
-  qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(qe, n, rows_per_tile, n_en, nb,
-                                                                StatePtrs<R>{}, 1, 1,
-                                                          reinterpret_cast<const C*>(W),
-                                                          c->partials.as<double>());
+  // mma kernels: warps of (state, kQeProjNT energy tiles), 8 per block
+  const dim3 pgrid_mma(
+      (unsigned)pgrid,
+      (unsigned)((nb * (((n_en + 7) / 8 + kQeProjNT - 1) / kQeProjNT) + kQeMmaWarps - 1) /
+                 kQeMmaWarps));
+  if (TBPM_QE_MMA)
+    qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, 0, c->stream>>>(
+        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
+        c->partials.as<double>());
+  else
+    qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(
+        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
+        c->partials.as<double>());
   TBPM_CK(cudaGetLastError());
   reduce_rows_kernel<<<(int)std::min<int64_t>(2 * n_ib, 65535), 256, 0, c->stream>>>(
       c->partials.as<double>(), pgrid, 2 * n_ib, c->small.as<double>());
@@ -1281,9 +1308,12 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       c->launches++;
       u.p[tau] = us;
     }
-    qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(qe, n, rows_per_tile, n_en,
-                                                                 nb, u, len, 0, nullptr,
-                                                                 c->partials.as<double>());
+    if (TBPM_QE_MMA)
+      qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, 0, c->stream>>>(
+          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
+    else
+      qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(
+          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
     TBPM_CK(cudaGetLastError());
     const int64_t n_vals = (int64_t)2 * len * 2 * n_ib;
     reduce_rows_kernel<<<(int)std::min<int64_t>(n_vals, 65535), 256, 0, c->stream>>>(
@@ -1924,11 +1954,18 @@ void drv_ac(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
 }
 
 
-void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
-            int seed, int rank, int n_ran_samples, int n_timestep, double t_step,
-            const double* energies, int n_energies, const int32_t* en_inds, int n_en_inds,
-            int chk_step, double chk_thr, double* dos_corr, double* dc_corr) {
+// The states [first_state, first_state + n_states) of a DC run of n_avg states:
+// their contributions, each divided by n_avg, are added to dos_corr / dc_corr
+// in state order (zeroed first when `zero`).  Seeded states (wf0 == NULL)
+// follow the seed rule with the run's n_ran_samples; wf0 holds this part's
+// states.
+void drv_dc_part(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int first_state,
+                 int n_states, int n_avg, int seed, int rank, int n_ran_samples, int n_timestep,
+                 double t_step, const double* energies, int n_energies, const int32_t* en_inds,
+                 int n_en_inds, int chk_step, double chk_thr, double* dos_corr, double* dc_corr,
+                 bool zero) {
   require_ham(c, true);
+  if (first_state < 0 || n_avg < 1) throw Error{TBPM_ERR_ARG, "bad state range"};
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
   if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
@@ -1943,8 +1980,10 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
   }
   c->launches = 0;
   c->model_bytes = 0;
-  std::fill(dos_corr, dos_corr + 2 * (size_t)n_timestep, 0.0);
-  std::fill(dc_corr, dc_corr + 2 * 2 * (size_t)n_energies * n_timestep, 0.0);
+  if (zero) {
+    std::fill(dos_corr, dos_corr + 2 * (size_t)n_timestep, 0.0);
+    std::fill(dc_corr, dc_corr + 2 * 2 * (size_t)n_energies * n_timestep, 0.0);
+  }
   const Expansion ex_fwd = time_step_expansion(bes, n_bes);
   // states per batch: the QE block (N x n_en x nb complex) must fit in memory.
   // When not even one state's block fits, the energies are taken in chunks:
@@ -1988,7 +2027,7 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
     StateKeys keys{};
     const StateKeys* kp = nullptr;
     if (!wf0) {
-      keys = make_keys(seed, s0 + 1, nb, rank, n_ran_samples);
+      keys = make_keys(seed, first_state + s0 + 1, nb, rank, n_ran_samples);
       kp = &keys;
     }
     const double* hw = wf0 ? wf0 + 2 * (size_t)s0 * c->ham.n : nullptr;
@@ -2000,12 +2039,21 @@ void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_
                [&](auto tag) {
                  using P = decltype(tag);
                  dc_batch<typename P::Real, P::V>(c, ex_pm, ex_fwd, nb, kp, hw, n_timestep,
-                                                  t_step, part, chk_step, chk_thr, n_states,
+                                                  t_step, part, chk_step, chk_thr, n_avg,
                                                   n_energies, dos_corr, dc_corr, nullptr,
                                                   "tbpm_dccond", e0, e0 == 0);
                });
     }
   }
+}
+
+void drv_dc(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
+            int seed, int rank, int n_ran_samples, int n_timestep, double t_step,
+            const double* energies, int n_energies, const int32_t* en_inds, int n_en_inds,
+            int chk_step, double chk_thr, double* dos_corr, double* dc_corr) {
+  drv_dc_part(c, bes, n_bes, wf0, 0, n_states, n_states, seed, rank, n_ran_samples, n_timestep,
+              t_step, energies, n_energies, en_inds, n_en_inds, chk_step, chk_thr, dos_corr,
+              dc_corr, true);
 }
 
 
@@ -2442,6 +2490,25 @@ void drv_session_export(tbpm_ctx* c, double* wf0, double* psi) {
     if (wf0) download_states<float>(c, c->wf0.p, ns, ns, 0, wf0);
     if (psi) download_states<float>(c, c->A.p, ns, ns, 0, psi);
   }
+}
+
+// One block waits, with the ring kernels' bounded wait, on an mbarrier phase
+// that nothing completes; the wait runs out after kRingWaitNs and records it
+// in the status word like any ring kernel would.
+__global__ void ring_wait_probe_kernel(unsigned int* status) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  const uint32_t b = ring_smem(&bar);
+  ring_bar_init(b, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if (!ring_wait(b, 0)) atomicOr(status, 1u);
+}
+
+void drv_selftest_wait_timeout(tbpm_ctx* c) {
+  ring_wait_probe_kernel<<<1, 32, 0, c->stream>>>(c->status.as<unsigned int>());
+  TBPM_CK(cudaGetLastError());
+  TBPM_CK(cudaStreamSynchronize(c->stream));
+  check_status(c);  // throws TBPM_ERR_TIMEOUT when the wait ran out
 }
 
 void drv_session_read(tbpm_ctx* c, double* corr, double* norms, int* n_done) {

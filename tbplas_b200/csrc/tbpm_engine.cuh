@@ -107,6 +107,7 @@ struct tbpm_ctx {
   tbpm::DevMem A, X, Y, wf0, partials, out, ctr, stage, small, qe, coef, seg;
   tbpm::DevMem raw;  // device copy of an uploaded host CSR, kept for the next upload
   tbpm::DevMem status;  // bit 0: a bounded device-side wait ran out (cleared when read)
+  tbpm::DevMem anl;     // inputs and outputs of the Analyzer's trigonometric sums
   int64_t launches = 0;
   double model_bytes = 0;
   tbpm::Session sess;

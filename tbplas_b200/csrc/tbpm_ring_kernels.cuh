@@ -44,10 +44,23 @@
 
 namespace tbpm {
 
-constexpr int kRingConsumerWarps = 7;
+#ifndef TBPM_RING_WARPS
+#define TBPM_RING_WARPS 7  // consumer warps per block
+#endif
+#ifndef TBPM_RING_MINB
+#define TBPM_RING_MINB 2  // resident blocks per SM the stages are sized for
+#endif
+#ifndef TBPM_RING_STAGES
+#define TBPM_RING_STAGES 8  // most stages per ring
+#endif
+#ifndef TBPM_RING_EVICT
+#define TBPM_RING_EVICT 0  // 1: bulk copies of p_{k-2} and the accumulator marked evict-first in L2
+#endif
+constexpr int kRingConsumerWarps = TBPM_RING_WARPS;
 constexpr int kRingConsumers = kRingConsumerWarps * 32;
 constexpr int kRingThreads = kRingConsumers + 32;
-constexpr int kRingMaxStages = 8;
+constexpr int kRingMaxStages = TBPM_RING_STAGES;
+constexpr int kRingMinBlocks = TBPM_RING_MINB;
 constexpr unsigned long long kRingWaitNs = 2000000000ull;  // 2 s per wait
 #ifndef TBPM_RING_GATHER
 #define TBPM_RING_GATHER 4  // neighbour gathers issued together
@@ -106,6 +119,22 @@ __device__ __forceinline__ void ring_copy(uint32_t dst, const void* src, uint32_
       : "memory");
 }
 
+// The same copy with an L2 eviction-priority policy (createpolicy).
+__device__ __forceinline__ void ring_copy_hint(uint32_t dst, const void* src, uint32_t bytes,
+                                               uint32_t bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+      "[%0], [%1], %2, [%3], %4;" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ uint64_t ring_evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // Wait for the phase of parity `parity` of mbarrier `bar`, at most kRingWaitNs.
 __device__ __forceinline__ bool ring_wait(uint32_t bar, uint32_t parity) {
   const unsigned long long t0 = ring_clock_ns();
@@ -130,7 +159,7 @@ __device__ __forceinline__ Pack<R, V> lds_pack(const char* p) {
 }
 
 template <typename R, int V, int MODE>
-__global__ void __launch_bounds__(kRingThreads, 2)
+__global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     cheb_ring_kernel(const __grid_constant__ RingArgs<R, V> ra) {
   using C = typename Cx<R>::t;
   extern __shared__ __align__(128) char rsm[];
@@ -233,9 +262,16 @@ __global__ void __launch_bounds__(kRingThreads, 2)
         }
         if (a.diag) ring_copy(ring_smem(st + sh.diag_off), a.diag + d0, d_bytes, bar);
         const int64_t e0 = r0 * tpr;
-        if (a.pin) ring_copy(ring_smem(st + sh.pin_off), a.pin + e0, tile, bar);
+        if (TBPM_RING_EVICT) {
+          // p_{k-2} and the accumulator are read once: keep L2 for p_{k-1}
+          const uint64_t pol = ring_evict_first_policy();
+          if (a.pin) ring_copy_hint(ring_smem(st + sh.pin_off), a.pin + e0, tile, bar, pol);
+          if (add_acc) ring_copy_hint(ring_smem(st + sh.acc_off), a.acc + e0, tile, bar, pol);
+        } else {
+          if (a.pin) ring_copy(ring_smem(st + sh.pin_off), a.pin + e0, tile, bar);
+          if (add_acc) ring_copy(ring_smem(st + sh.acc_off), a.acc + e0, tile, bar);
+        }
         if (need_own) ring_copy(ring_smem(st + sh.own_off), a.gather + e0, tile, bar);
-        if (add_acc) ring_copy(ring_smem(st + sh.acc_off), a.acc + e0, tile, bar);
       }
       __syncwarp();
       ++issued;

@@ -44,11 +44,39 @@ def _window_values(window: Callable, start: int, stop: int, tnr: int) -> np.ndar
     return np.array([window(i, tnr) for i in range(start, stop)], dtype=float)
 
 
+def _trig_sums(ctx, w, a, b, x, dt, per_output: bool, phase_kdt: bool):
+    """tbpm_trig_sums: (sum_k w a cos, sum_k w b sin) for every row of a / b
+    (leading axes) and every x; either coefficient array may be None."""
+    from .. import _native as nat
+    w = np.ascontiguousarray(w, dtype=float)
+    x = np.ascontiguousarray(x, dtype=float)
+    ref = a if a is not None else b
+    lead = ref.shape[:-2] if per_output else ref.shape[:-1]
+    n_rows = int(np.prod(lead)) if len(lead) else 1
+    shape = tuple(lead) + (x.size,)
+    a = None if a is None else np.ascontiguousarray(a, dtype=float)
+    b = None if b is None else np.ascontiguousarray(b, dtype=float)
+    oc = np.zeros(shape) if a is not None else None
+    os_ = np.zeros(shape) if b is not None else None
+    ctx.call("tbpm_trig_sums", nat.ptr(w), w.size, nat.ptr(a), nat.ptr(b), n_rows, nat.ptr(x),
+             x.size, float(dt), 1 if per_output else 0, 1 if phase_kdt else 0, nat.ptr(oc),
+             nat.ptr(os_))
+    return oc, os_
+
+
 class Analyzer(MPIEnv):
-    """Post-processing of TBPM correlation functions (see tbplas.tbpm.Analyzer)."""
+    """Post-processing of TBPM correlation functions (see tbplas.tbpm.Analyzer).
+
+    The trigonometric sums of calc_ac_cond, calc_dyn_pol, calc_dc_cond and
+    calc_diff_coeff run on the GPU (tbpm_trig_sums, tbpm_trig_cumtrapz) when
+    `backend` is "gpu", or "auto" and a GPU is visible; backend "host" (or
+    "auto" without a GPU, e.g. post-processing saved correlations on a
+    workstation) evaluates the same formulas with numpy.
+    """
 
     def __init__(self, sample, config: Config, dimension: int = 3,
-                 enable_mpi: bool = False, echo_details: bool = False) -> None:
+                 enable_mpi: bool = False, echo_details: bool = False,
+                 backend: str = "auto") -> None:
         super().__init__(enable_mpi=enable_mpi, echo_details=echo_details)
         self._sample = sample
         self._config = config
@@ -56,6 +84,25 @@ class Analyzer(MPIEnv):
         if dimension not in (2, 3):
             raise ValueError(f"Unsupported dimension: {dimension}")
         self._dimension = dimension
+        if backend not in ("auto", "gpu", "host"):
+            raise ValueError(f"Unsupported backend: {backend}")
+        self._backend = backend
+        self._dev = None
+
+    def _device(self):
+        """The library context the sums run on, or None for numpy."""
+        if self._backend == "host":
+            return None
+        if self._dev is None:
+            from .. import _native as nat
+            try:
+                self._dev = nat.get_context()
+            except Exception:
+                if self._backend == "gpu":
+                    raise
+                self._backend = "host"
+                return None
+        return self._dev
 
     def _energies(self) -> np.ndarray:
         tnr = self._config.generic['nr_time_steps']
@@ -118,10 +165,16 @@ class Analyzer(MPIEnv):
         if self.is_master:
             corr = np.asarray(corr_ac)
             w = _window_values(window, 1, tnr + 1, tnr)
-            k = np.arange(tnr, dtype=float)
-            # S[i, k] = 2 w(k+1) sin(omega_i k dt)
-            s = 2. * w[None, :] * np.sin(np.outer(omegas, k) * t_step)
-            acv = s @ np.imag(corr[:, :tnr]).T  # (tnr, 4)
+            dev = self._device()
+            if dev is not None:
+                _, ssum = _trig_sums(dev, w, None, np.imag(corr[:, :tnr]), omegas, t_step,
+                                     per_output=False, phase_kdt=False)
+                acv = 2. * ssum.T  # (tnr, 4)
+            else:
+                k = np.arange(tnr, dtype=float)
+                # S[i, k] = 2 w(k+1) sin(omega_i k dt)
+                s = 2. * w[None, :] * np.sin(np.outer(omegas, k) * t_step)
+                acv = s @ np.imag(corr[:, :tnr]).T  # (tnr, 4)
             with np.errstate(divide="ignore", invalid="ignore"):
                 fac = prefactor * t_step * (np.exp(-beta * omegas) - 1) / omegas
             fac[omegas == 0.] = 0.
@@ -167,12 +220,19 @@ class Analyzer(MPIEnv):
         dc = np.zeros((2, n_energies))
         if self.is_master:
             w = _window_values(window_dc, 1, tnr + 1, tnr)
-            k = np.arange(tnr, dtype=float)
-            phi = np.outer(energies, k) * t_step  # (n_en, tnr)
-            c_exp = np.cos(phi) - 1j * np.sin(phi)
             corr = np.asarray(corr_dc)[:, :n_energies, :tnr]
-            vals = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
-            dc_val = vals.sum(axis=2)
+            dev = self._device()
+            if dev is not None and n_energies > 0:
+                # Re(exp(-i E k dt) c) = Re(c) cos + Im(c) sin
+                csum, ssum = _trig_sums(dev, w, np.real(corr), np.imag(corr), energies, t_step,
+                                        per_output=True, phase_kdt=False)
+                dc_val = csum + ssum
+            else:
+                k = np.arange(tnr, dtype=float)
+                phi = np.outer(energies, k) * t_step  # (n_en, tnr)
+                c_exp = np.cos(phi) - 1j * np.sin(phi)
+                vals = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
+                dc_val = vals.sum(axis=2)
             dc = prefactor * t_step * dos[qe_indices][None, :] * dc_val
             if self._config.generic['correct_spin']:
                 dc = 2. * dc
@@ -195,12 +255,25 @@ class Analyzer(MPIEnv):
         diff_coeff = np.zeros((2, n_energies, tnr))
         if self.is_master:
             w = _window_values(window_dc, 1, tnr + 1, tnr)
-            k = np.arange(tnr, dtype=float)
-            phi = np.outer(energies, k) * t_step
-            c_exp = np.cos(phi) - 1j * np.sin(phi)
             corr = np.asarray(corr_dc)[:, :n_energies, :tnr]
-            temp = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
-            diff_coeff[:, :, 1:] = cumulative_trapezoid(temp, time, axis=2)
+            dev = self._device()
+            if dev is not None and n_energies > 0:
+                from .. import _native as nat
+                a = np.ascontiguousarray(np.real(corr))
+                b = np.ascontiguousarray(np.imag(corr))
+                x = np.ascontiguousarray(np.tile(energies, 2))
+                spacing = np.ascontiguousarray(np.diff(time))
+                out = np.zeros((2, n_energies, tnr))
+                dev.call("tbpm_trig_cumtrapz", nat.ptr(w), tnr, nat.ptr(a), nat.ptr(b),
+                         2 * n_energies, nat.ptr(x), float(t_step), nat.ptr(spacing),
+                         nat.ptr(out))
+                diff_coeff = out
+            else:
+                k = np.arange(tnr, dtype=float)
+                phi = np.outer(energies, k) * t_step
+                c_exp = np.cos(phi) - 1j * np.sin(phi)
+                temp = np.real(c_exp[None, :, :] * corr) * w[None, None, :]
+                diff_coeff[:, :, 1:] = cumulative_trapezoid(temp, time, axis=2)
         self.bcast(diff_coeff)
         return time, diff_coeff
 
@@ -225,11 +298,17 @@ class Analyzer(MPIEnv):
         dyn_pol = np.zeros((len(q_points), tnr), dtype=complex)
         if self.is_master:
             w = _window_values(window, 1, tnr + 1, tnr)
-            k = np.arange(tnr, dtype=float)
-            phi = np.outer(omegas, k * t_step)  # phi[i, k] = k*dt*omega_i
-            e = np.cos(phi) + 1j * np.sin(phi)
             corr = np.asarray(corr_dyn_pol, dtype=float)[:, :tnr]
-            dyn_pol = prefactor * t_step * ((corr * w[None, :]) @ e.T)
+            dev = self._device()
+            if dev is not None:
+                csum, ssum = _trig_sums(dev, w, corr, corr, omegas, t_step, per_output=False,
+                                        phase_kdt=True)
+                dyn_pol = prefactor * t_step * (csum + 1j * ssum)
+            else:
+                k = np.arange(tnr, dtype=float)
+                phi = np.outer(omegas, k * t_step)  # phi[i, k] = k*dt*omega_i
+                e = np.cos(phi) + 1j * np.sin(phi)
+                dyn_pol = prefactor * t_step * ((corr * w[None, :]) @ e.T)
             if self._config.generic['correct_spin']:
                 dyn_pol = 2. * dyn_pol
         self.bcast(dyn_pol)

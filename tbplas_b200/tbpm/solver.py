@@ -38,7 +38,8 @@ class Solver(MPIEnv):
     :param checkpoint: optional {'path': file, 'every': time steps}: calc_corr_dos
         writes its state to path every `every` steps and resumes from it when
         called again with the same inputs (tbplas_b200.checkpoint); each rank
-        uses path + '.rank<r>'
+        uses path + '.rank<r>'.  calc_corr_dc_cond writes path + '.dc' after every
+        'states_per_part' states (default: the batch width) and resumes from it
     :param kwargs: arguments of set_output
     """
 
@@ -226,13 +227,26 @@ class Solver(MPIEnv):
         indptr, indices, hop, dx, dy = self._sample.build_ham_dxy()
         num_sample = self._dist_sample()
         self._echo_time_step_fs(time_step)
-        corr_dos, corr_dc = f2py.tbpm_dccond(
-            bessel_series, beta_re, mu_re, indptr, indices, hop,
-            self._sample.rescale, dx, dy,
-            self._config.generic['seed'], self._config.generic['nr_time_steps'], num_sample,
-            time_step, energies_dos, qe_indices,
-            self._output['corr_DOS'], self._output['corr_DC'], self.rank,
-            self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
+        if self._checkpoint:
+            from ..checkpoint import dc_checkpointed
+            path = self._checkpoint["path"] + ".dc"
+            if self.size > 1:
+                path = f"{path}.rank{self.rank}"
+            corr_dos, corr_dc = dc_checkpointed(
+                bessel_series, indptr, indices, hop, self._sample.rescale, dx, dy,
+                self._config.generic['seed'], self._config.generic['nr_time_steps'],
+                num_sample, time_step, energies_dos, qe_indices, self.rank,
+                self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'],
+                path, states_per_part=self._checkpoint.get("states_per_part"),
+                on_checkpoint=self._checkpoint.get("on_dc_checkpoint"))
+        else:
+            corr_dos, corr_dc = f2py.tbpm_dccond(
+                bessel_series, beta_re, mu_re, indptr, indices, hop,
+                self._sample.rescale, dx, dy,
+                self._config.generic['seed'], self._config.generic['nr_time_steps'], num_sample,
+                time_step, energies_dos, qe_indices,
+                self._output['corr_DOS'], self._output['corr_DC'], self.rank,
+                self._config.generic['wfn_check_steps'], self._config.generic['wfn_check_thr'])
         corr_dos = self.all_average(corr_dos)
         corr_dc = self.all_average(corr_dc)
         self._save_data(corr_dos, self._output["corr_DOS"])

@@ -94,3 +94,40 @@ def test_fp32_resume_and_solver_checkpoint(tmp_path, ham):
                   checkpoint={"path": str(tmp_path / "solver.npz"), "every": 8})
     b = tb.Solver(s, cfg, echo_details=False, directory=str(tmp_path), prefix="b")
     assert np.array_equal(a.calc_corr_dos(), b.calc_corr_dos())
+
+
+@pytest.mark.parametrize("stop_after", [2, 4])
+def test_dc_resume_reproduces_uninterrupted_run(tmp_path, stop_after):
+    """DC (tbpm_dccond) checkpointed between parts of two states: stopped after
+    the first or second part and resumed, the result is bit-identical to the
+    same run without interruption, and equals one tbpm_dccond call to the
+    FP64 bar."""
+    from tbplas_b200.checkpoint import dc_checkpointed
+    s = tb.make_graphene_sample(10, 8, disorder=0.8, rescale=9.0, seed=5)
+    ip, ix, hv, dx, dy = s.build_ham_dxy()
+    tnr = 24
+    en_range = s.energy_range
+    energies = np.array([0.5 * i * en_range / tnr - en_range / 2. for i in range(2 * tnr)])
+    sel = np.where((energies >= -2.0) & (energies <= 2.0))[0]
+    bes = bessel_series(math.pi)
+    t_step = 2 * math.pi / en_range
+    args = (bes, ip, ix, hv, s.rescale, dx, dy, 1337, tnr, 5, t_step, energies, sel, 0, 16,
+            1e-9)
+    whole = dc_checkpointed(*args, str(tmp_path / "whole.npz"), states_per_part=2)
+    path = str(tmp_path / "dc.npz")
+
+    def cb(done):
+        if done == stop_after:
+            raise Stop()
+
+    with pytest.raises(Stop):
+        dc_checkpointed(*args, path, states_per_part=2, on_checkpoint=cb)
+    assert os.path.exists(path)
+    got = dc_checkpointed(*args, path, states_per_part=2)
+    assert not os.path.exists(path)
+    for k in (0, 1):
+        assert np.array_equal(got[k], whole[k])
+    ref = f2py.tbpm_dccond(bes, 0.0, 0.0, ip, ix, hv, s.rescale, dx, dy, 1337, tnr, 5, t_step,
+                           energies, sel, "", "", 0, 16, 1e-9)
+    for k in (0, 1):
+        assert rel_err(got[k], ref[k]) < 1e-12

@@ -387,3 +387,20 @@ def test_nan_initial_state_reports_nan_status(graphene_small, dos_bes, driver):
     # the context stays usable
     got = f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0[:1], 8, 4, 1e-9)
     assert rel_err(got, oracle.tbpm_dos(dos_bes, ip, ix, hv, 8, wf0=wf0[:1])) < FP64_TOL
+
+
+def test_bounded_wait_runs_out_reports_timeout_and_context_stays_usable(graphene_small,
+                                                                          dos_bes):
+    """A device wait on a barrier that nothing completes gives up after its
+    bound and the call returns TBPM_ERR_TIMEOUT; the next propagation on the
+    same context is correct."""
+    ctx = f2py._ctx()
+    import time
+    t0 = time.perf_counter()
+    with pytest.raises(nat.DeviceTimeoutError):
+        ctx.call("tbpm_selftest_wait_timeout")
+    assert time.perf_counter() - t0 < 30
+    ip, ix, hv = _csr(graphene_small)
+    wf0 = unit_states(2, ip.size - 1, seed=9)
+    got = f2py.tbpm_dos_states(dos_bes, ip, ix, hv, wf0, 8, 4, 1e-9)
+    assert rel_err(got, oracle.tbpm_dos(dos_bes, ip, ix, hv, 8, wf0=wf0)) < FP64_TOL
