@@ -525,7 +525,8 @@ __global__ void __launch_bounds__(256, TBPM_QE_MINB_P) qe_project_kernel(
 // time (one k-step of mma.sync m8n8k4 f64): 4 A fragments (from u, shared by
 // its energy tiles) and one B fragment per energy tile (QE) per step.  The
 // block partials have the layout of qe_project_kernel.
-constexpr int kQeProjNT = 4;
+constexpr int kQeProjNT = 2;  // energy tiles (of 8) per warp
+constexpr int kQeProjKS = 4;  // k-steps (row pairs) whose loads are issued together
 
 template <typename R>
 __global__ void __launch_bounds__(kQeMmaWarps * 32, 2) qe_project_mma_kernel(
@@ -547,52 +548,65 @@ __global__ void __launch_bounds__(kQeMmaWarps * 32, 2) qe_project_mma_kernel(
   if (task >= nb * groups) return;
   const int b = task % nb;
   const int nt0 = (task / nb) * kQeProjNT;
+  const int part = t & 1;
+  // per M-tile: the u column of this lane's row mm = 8*mt + g (m = mm / 2)
+  const C* ucol[4];
+  int useg[4];  // 0: unused row, 1: c = re, 2: c = im
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int mm = 8 * mt + g;
+    const int m = mm >> 1;
+    useg[mt] = m < M ? 1 + (mm & 1) : 0;
+    if (mode == 0) {
+      const int tau = m < M ? m / K : 0, k = m < M ? m - (m / K) * K : 0;
+      ucol[mt] = u.p[tau] + k * nb + b;
+    } else {
+      ucol[mt] = wf0 + b;
+    }
+  }
+  const int64_t ustride = mode == 0 ? ld : nb;
   double acc[4][kQeProjNT][2];
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int j = 0; j < kQeProjNT; ++j) acc[mt][j][0] = acc[mt][j][1] = 0.0;
-  for (int64_t rp = r0; rp < r1; rp += 2) {
-    // k index 4*0 + t: row rp + t/2, part t&1
-    const int64_t r = rp + (t >> 1);
-    const bool rok = r < r1;
-    const int part = t & 1;
-    double afr[4];
+  for (int64_t rp = r0; rp < r1; rp += 2 * kQeProjKS) {
+    double afr[kQeProjKS][4], bfr[kQeProjKS][kQeProjNT];
+    // all loads of kQeProjKS row pairs first: row rp + 2s + t/2, part t&1
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-      const int mm = 8 * mt + g;
-      const int m = mm >> 1, c = mm & 1;
-      double v = 0.0;
-      if (rok && m < M) {
-        C w;
-        if (mode == 0) {
-          const int tau = m / K, k = m - tau * K;
-          w = u.p[tau][r * ld + k * nb + b];
-        } else {
-          w = wf0[r * nb + b];
+    for (int st = 0; st < kQeProjKS; ++st) {
+      const int64_t r = rp + 2 * st + (t >> 1);
+      const bool rok = r < r1;
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        double v = 0.0;
+        if (rok && useg[mt]) {
+          const C w = ucol[mt][r * ustride];
+          const double ur = (double)w.x, ui = (double)w.y;
+          v = useg[mt] == 1 ? (part == 0 ? ur : ui) : (part == 0 ? -ui : ur);
         }
-        const double ur = (double)w.x, ui = (double)w.y;
-        v = c == 0 ? (part == 0 ? ur : ui) : (part == 0 ? -ui : ur);
+        afr[st][mt] = v;
       }
-      afr[mt] = v;
-    }
-    double bfr[kQeProjNT];
 #pragma unroll
-    for (int j = 0; j < kQeProjNT; ++j) {
-      const int i = (nt0 + j) * 8 + g;
-      double v = 0.0;
-      if (rok && i < n_en) {
-        const C q = qe[(r * n_en + i) * nb + b];
-        v = part == 0 ? (double)q.x : (double)q.y;
+      for (int j = 0; j < kQeProjNT; ++j) {
+        const int i = (nt0 + j) * 8 + g;
+        double v = 0.0;
+        if (rok && i < n_en) {
+          const C q = qe[(r * n_en + i) * nb + b];
+          v = part == 0 ? (double)q.x : (double)q.y;
+        }
+        bfr[st][j] = v;
       }
-      bfr[j] = v;
     }
 #pragma unroll
-    for (int j = 0; j < kQeProjNT; ++j)
-      if (nt0 + j < n_nt) {
+    for (int st = 0; st < kQeProjKS; ++st)
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) dmma_8x8x4(acc[mt][j][0], acc[mt][j][1], afr[mt], bfr[j]);
-      }
+      for (int j = 0; j < kQeProjNT; ++j)
+        if (nt0 + j < n_nt) {
+#pragma unroll
+          for (int mt = 0; mt < 4; ++mt)
+            dmma_8x8x4(acc[mt][j][0], acc[mt][j][1], afr[st][mt], bfr[st][j]);
+        }
   }
   // C[mm][n]: lane holds rows mm = 8*mt + g, columns n = 2t, 2t+1 (energies)
 #pragma unroll
