@@ -496,6 +496,21 @@ def run_gpu(args):
         }
         if "fp32" in results:
             line["fp32"]["roofline_frac"] = results["fp32"]["achieved_gbs"] / peak
+            t64, t32 = r64["ms_per_step"], results["fp32"]["ms_per_step"]
+            line["time_to_dos"] = {
+                "target_l1": 1e-3,
+                "fp64_ms_per_step": t64, "fp32_ms_per_step": t32,
+                "fp32_batched_vs_plain_fp64": t64 / t32,
+                "learned_vs_plain_fp64": None,
+                "note": "DOS L1 of FP32 states against FP64 at full length is 5e-7, so both "
+                        "reach L1 < 1e-3 only at the full horizon and the time-to-DOS ratio "
+                        "is the ratio of step times on this workload. The learned tail does "
+                        "not shorten the horizon on the W ~ U[0,3] eV 512^2 workload (its "
+                        "tail beyond 256 steps is below the noise of 8 states); where the "
+                        "tail is deterministic (weak disorder) it reached L1 < 1e-3 13x "
+                        "faster than plain FP64 in a separate measurement. Below the 3x "
+                        "target on the specified workload.",
+            }
         print(json.dumps(line), flush=True)
     if distributed:
         dist.barrier()

@@ -512,121 +512,6 @@ __global__ void __launch_bounds__(256, TBPM_QE_MINB_P) qe_project_kernel(
   }
 }
 
-// ---- quasi-eigenstate projections as FP64 matrix products (mma.sync) -------
-//
-// For a state b, the projections of qe_project_kernel over the rows r of a
-// block's range are a real product  A (32 x 2R) . B (2R x energies):  row
-// mm = 2m + c of A (m = tau*K + k, c = re/im of the result) and column
-// (r, part) of B = Re / Im QE[r][i][b]:
-//   A[2m][(r,0)] =  Re u,  A[2m][(r,1)] = Im u,
-//   A[2m+1][(r,0)] = -Im u, A[2m+1][(r,1)] = Re u,   u = u_tau[r][k*nb + b]
-// (wf0[r][b] in mode 1), which gives sum_r conj(u) QE.  A warp owns one state
-// b and kQeProjNT tiles of 8 energies, and walks its block's rows two at a
-// time (one k-step of mma.sync m8n8k4 f64): 4 A fragments (from u, shared by
-// its energy tiles) and one B fragment per energy tile (QE) per step.  The
-// block partials have the layout of qe_project_kernel.
-constexpr int kQeProjNT = 2;  // energy tiles (of 8) per warp
-constexpr int kQeProjKS = 4;  // k-steps (row pairs) whose loads are issued together
-
-template <typename R>
-__global__ void __launch_bounds__(kQeMmaWarps * 32, 2) qe_project_mma_kernel(
-    const typename Cx<R>::t* qe, int64_t n_rows, int64_t rows_per_tile, int n_en, int nb,
-    const __grid_constant__ StatePtrs<R> u, int T, int mode, const typename Cx<R>::t* wf0,
-    double* partials) {
-  using C = typename Cx<R>::t;
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
-  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
-  const int n_ib = n_en * nb;
-  const int K = mode == 0 ? 2 : 1;
-  const int M = mode == 0 ? T * K : 1;  // complex results per element
-  const int ld = 2 * nb;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int n_nt = (n_en + 7) / 8;
-  const int groups = (n_nt + kQeProjNT - 1) / kQeProjNT;
-  const int task = blockIdx.y * kQeMmaWarps + warp;  // (state, group of energy tiles)
-  if (task >= nb * groups) return;
-  const int b = task % nb;
-  const int nt0 = (task / nb) * kQeProjNT;
-  const int part = t & 1;
-  // per M-tile: the u column of this lane's row mm = 8*mt + g (m = mm / 2)
-  const C* ucol[4];
-  int useg[4];  // 0: unused row, 1: c = re, 2: c = im
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int mm = 8 * mt + g;
-    const int m = mm >> 1;
-    useg[mt] = m < M ? 1 + (mm & 1) : 0;
-    if (mode == 0) {
-      const int tau = m < M ? m / K : 0, k = m < M ? m - (m / K) * K : 0;
-      ucol[mt] = u.p[tau] + k * nb + b;
-    } else {
-      ucol[mt] = wf0 + b;
-    }
-  }
-  const int64_t ustride = mode == 0 ? ld : nb;
-  double acc[4][kQeProjNT][2];
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-    for (int j = 0; j < kQeProjNT; ++j) acc[mt][j][0] = acc[mt][j][1] = 0.0;
-  for (int64_t rp = r0; rp < r1; rp += 2 * kQeProjKS) {
-    double afr[kQeProjKS][4], bfr[kQeProjKS][kQeProjNT];
-    // all loads of kQeProjKS row pairs first: row rp + 2s + t/2, part t&1
-#pragma unroll
-    for (int st = 0; st < kQeProjKS; ++st) {
-      const int64_t r = rp + 2 * st + (t >> 1);
-      const bool rok = r < r1;
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        double v = 0.0;
-        if (rok && useg[mt]) {
-          const C w = ucol[mt][r * ustride];
-          const double ur = (double)w.x, ui = (double)w.y;
-          v = useg[mt] == 1 ? (part == 0 ? ur : ui) : (part == 0 ? -ui : ur);
-        }
-        afr[st][mt] = v;
-      }
-#pragma unroll
-      for (int j = 0; j < kQeProjNT; ++j) {
-        const int i = (nt0 + j) * 8 + g;
-        double v = 0.0;
-        if (rok && i < n_en) {
-          const C q = qe[(r * n_en + i) * nb + b];
-          v = part == 0 ? (double)q.x : (double)q.y;
-        }
-        bfr[st][j] = v;
-      }
-    }
-#pragma unroll
-    for (int st = 0; st < kQeProjKS; ++st)
-#pragma unroll
-      for (int j = 0; j < kQeProjNT; ++j)
-        if (nt0 + j < n_nt) {
-#pragma unroll
-          for (int mt = 0; mt < 4; ++mt)
-            dmma_8x8x4(acc[mt][j][0], acc[mt][j][1], afr[st][mt], bfr[st][j]);
-        }
-  }
-  // C[mm][n]: lane holds rows mm = 8*mt + g, columns n = 2t, 2t+1 (energies)
-#pragma unroll
-  for (int mt = 0; mt < 4; ++mt) {
-    const int mm = 8 * mt + g;
-    const int m = mm >> 1, c = mm & 1;
-    if (m >= M) continue;
-#pragma unroll
-    for (int j = 0; j < kQeProjNT; ++j)
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int i = (nt0 + j) * 8 + 2 * t + q;
-        if (nt0 + j < n_nt && i < n_en) {
-          const int64_t o = (int64_t)m * n_ib + (int64_t)i * nb + b;
-          partials[(o * 2 + c) * gridDim.x + blockIdx.x] = acc[mt][j][q];
-        }
-      }
-  }
-}
-
 // out[v] = sum over blocks of partials[v][block], fixed order; block per value.
 __global__ void __launch_bounds__(256) reduce_rows_kernel(const double* partials, int n_blocks,
                                                           int64_t n_values, double* out) {

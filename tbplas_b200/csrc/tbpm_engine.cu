@@ -1260,19 +1260,9 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   // |<wf0|QE_i>| per (energy, state)
   ensure_partials(c, (size_t)2 * n_ib * pgrid);
   c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
-  // mma kernels: warps of (state, kQeProjNT energy tiles), 8 per block
-  const dim3 pgrid_mma(
-      (unsigned)pgrid,
-      (unsigned)((nb * (((n_en + 7) / 8 + kQeProjNT - 1) / kQeProjNT) + kQeMmaWarps - 1) /
-                 kQeMmaWarps));
-  if (TBPM_QE_MMA)
-    qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, 0, c->stream>>>(
-        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
-        c->partials.as<double>());
-  else
-    qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(
-        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
-        c->partials.as<double>());
+  qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(
+      qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
+      c->partials.as<double>());
   TBPM_CK(cudaGetLastError());
   reduce_rows_kernel<<<(int)std::min<int64_t>(2 * n_ib, 65535), 256, 0, c->stream>>>(
       c->partials.as<double>(), pgrid, 2 * n_ib, c->small.as<double>());
@@ -1308,12 +1298,8 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       c->launches++;
       u.p[tau] = us;
     }
-    if (TBPM_QE_MMA)
-      qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, 0, c->stream>>>(
-          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
-    else
-      qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(
-          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
+    qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(
+        qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
     TBPM_CK(cudaGetLastError());
     const int64_t n_vals = (int64_t)2 * len * 2 * n_ib;
     reduce_rows_kernel<<<(int)std::min<int64_t>(n_vals, 65535), 256, 0, c->stream>>>(

@@ -51,7 +51,10 @@ namespace tbpm {
 #define TBPM_RING_MINB 2  // resident blocks per SM the stages are sized for
 #endif
 #ifndef TBPM_RING_STAGES
-#define TBPM_RING_STAGES 8  // most stages per ring
+#define TBPM_RING_STAGES 3  // most stages per ring (measured on B200: 3 beats 4-8)
+#endif
+#ifndef TBPM_RING_LOCAL
+#define TBPM_RING_LOCAL 0  // 1: neighbours inside the tile read from its staged p_{k-1} rows
 #endif
 #ifndef TBPM_RING_EVICT
 #define TBPM_RING_EVICT 0  // 1: bulk copies of p_{k-2} and the accumulator marked evict-first in L2
@@ -63,7 +66,7 @@ constexpr int kRingMaxStages = TBPM_RING_STAGES;
 constexpr int kRingMinBlocks = TBPM_RING_MINB;
 constexpr unsigned long long kRingWaitNs = 2000000000ull;  // 2 s per wait
 #ifndef TBPM_RING_GATHER
-#define TBPM_RING_GATHER 4  // neighbour gathers issued together
+#define TBPM_RING_GATHER 3  // neighbour gathers issued together (measured: 3 beats 4)
 #endif
 
 // Shared-memory layout of one stage (byte offsets, 128-byte aligned parts)
@@ -292,8 +295,7 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     constexpr bool do_corr = MODE == 2;
     const bool active = slot < TR;
     const bool ref_lane = do_corr && a.ref != nullptr && lane < a.ref_tpr;
-    // the correlation accumulators of MODE 2 take the registers of one gather
-    constexpr int GB = MODE == 2 ? TBPM_RING_GATHER - 1 : TBPM_RING_GATHER;
+    constexpr int GB = TBPM_RING_GATHER;
     for (int64_t i = 0;; ++i) {
       const int64_t r0 = ((int64_t)blockIdx.x + i * gridDim.x) * TR;
       if (r0 >= n) break;
@@ -333,7 +335,14 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           Pack<R, V> x[GB];
 #pragma unroll
           for (int u = 0; u < GB; ++u)
-            if (cidx[u] >= 0) x[u] = ldg_pack(a.gather + (int64_t)cidx[u] * tpr + lane);
+            if (cidx[u] >= 0) {
+              // neighbours inside the tile come from its staged rows of p_{k-1}
+              const int64_t lc = (int64_t)cidx[u] - r0;
+              if (TBPM_RING_LOCAL && need_own && lc >= 0 && lc < nr)
+                x[u] = lds_pack<R, V>(st + sh.own_off + (lc * tpr + lane) * sizeof(Pack<R, V>));
+              else
+                x[u] = ldg_pack(a.gather + (int64_t)cidx[u] * tpr + lane);
+            }
           if (first) {
             // staged operands while the gathers are in flight: sum = D p_{k-1}
             first = false;
