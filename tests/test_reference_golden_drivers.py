@@ -114,3 +114,23 @@ def test_hall_trace_oracle_matches_reference(g):
 def test_device_sample_positions_match_reference(g):
     d = tb.make_graphene_device_sample(8, 7, rescale=9.0)
     assert np.array_equal(d.orb_pos, g["orb_pos"])
+
+
+def test_recorded_reference_solver_calls_replay_on_the_oracle():
+    """tests/golden/reference_calls.npz (the reference Solver's own f2py calls,
+    see make_golden_calls.py) replays through the oracle's f2py-compatible
+    shim to the recorded results: the fixture and the oracle agree, so the GPU
+    replay of the same calls checks the drop-in against the oracle."""
+    calls_path = os.path.join(os.path.dirname(__file__), "golden", "reference_calls.npz")
+    gc = np.load(calls_path)
+    shim = oracle.F2pyShim()
+    for k, name in enumerate(gc["calls"]):
+        args = []
+        for i, kind in enumerate(gc[f"call{k}/kinds"]):
+            v = gc[f"call{k}/arg{i}"]
+            args.append(v if kind == "array" else v.tolist() if kind == "list" else
+                        str(v) if kind == "str" else int(v) if kind == "int" else float(v))
+        got = getattr(shim, str(name))(*args)
+        got = got if isinstance(got, tuple) else (got,)
+        for j in range(int(gc[f"call{k}/n_results"])):
+            assert np.array_equal(got[j], gc[f"call{k}/result{j}"]), (name, j)
