@@ -527,6 +527,10 @@ def main(argv=None) -> None:
                     help="override the number of time steps (shorter runs)")
     ap.add_argument("--out", default=None)
     ap.add_argument("--data", default=None, help="c4: npz cache of the generated curves")
+    ap.add_argument("--n-train", type=int, default=None,
+                    help="c4: training realisations (curves = realisations x states)")
+    ap.add_argument("--n-states", type=int, default=None,
+                    help="c4: states per realisation (training and test)")
     ap.add_argument("--builder", default="device", choices=["device", "host"],
                     help="c5: assemble the Hamiltonian on the GPU or on the host")
     ap.add_argument("--nx", type=int, default=None,
@@ -542,6 +546,10 @@ def main(argv=None) -> None:
                  {"steps_dos": args.steps, "steps_ac": args.steps}
         if w == "c4" and args.data:
             kw["data"] = args.data
+        if w == "c4" and args.n_train:
+            kw["n_train"] = args.n_train
+        if w == "c4" and args.n_states:
+            kw["n_states"] = args.n_states
         if w == "c5":
             kw["builder"] = args.builder
             if args.nx:
