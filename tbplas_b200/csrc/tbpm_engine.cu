@@ -254,11 +254,12 @@ struct TermTiles {
   RingShape rs[3] = {};
 };
 
-// Ring layout for rows of tpr packs in kernel mode `mode`; stages == 0 when the
-// ring does not apply (rows that are not a multiple of 16 bytes, or a stage
-// that does not fit twice into half of an SM's shared memory).
+// Ring layout for rows of tpr packs in kernel mode `mode` (ref_tpr: packs per
+// row of the MODE 2 correlation reference, 0 for none); stages == 0 when the
+// ring does not apply (rows that are not a multiple of 16 bytes, or fewer than
+// two stages fit into the shared memory of one of kRingMinBlocks blocks per SM).
 template <typename R, int V>
-RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode) {
+RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode, int ref_tpr) {
   RingShape s{};
   const size_t row_bytes = (size_t)tpr * sizeof(Pack<R, V>);
   if (row_bytes % 16 != 0 || tpr < 1 || tpr > kRingConsumers) return s;
@@ -291,6 +292,13 @@ RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode) {
   off += al((size_t)cap * 4);
   s.hop_off = off;
   off += al((size_t)cap * cs);
+  // MODE 2: the correlation reference's rows too, when they are whole 16-byte units
+  s.ref_off = -1;
+  const size_t ref_row = (size_t)ref_tpr * sizeof(Pack<R, V>);
+  if (mode == 2 && ref_tpr > 0 && ref_row % 16 == 0) {
+    s.ref_off = off;
+    off += al((size_t)TR * ref_row);
+  }
   s.stage_bytes = off;
   // kRingMinBlocks resident blocks per SM (228 KB of shared memory, 1 KB
   // reserved per block)
@@ -323,7 +331,7 @@ int ring_blocks_per_sm(const tbpm_ctx* c, const RingShape& rs) {
 #define TBPM_F32V4_THREADS 128
 #endif
 template <typename R, int V>
-TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr) {
+TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr, int ref_tpr = 0) {
   TermTiles tt;
   // measured on B200 (2048^2 graphene, 16 states): 128-thread blocks for FP64,
   // 256 for FP32
@@ -333,7 +341,7 @@ TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr) {
   tt.t[2] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 2>, V * 3 * sizeof(double), th);
   if (c->opts.term_kernel != 1) {
     for (int m = 0; m < 3; ++m) {
-      const RingShape rs = ring_shape<R, V>(c, tpr, m);
+      const RingShape rs = ring_shape<R, V>(c, tpr, m, ref_tpr);
       if (rs.stages == 0) continue;
       const int per_sm = m == 0   ? ring_blocks_per_sm<R, V, 0>(c, rs)
                          : m == 1 ? ring_blocks_per_sm<R, V, 1>(c, rs)
@@ -394,7 +402,7 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
   if (!A_out) A_out = A;
   const Ham& h = c->ham;
   const int tpr = ld / V;
-  const TermTiles tt = term_tiles<R, V>(c, h.n, tpr);
+  const TermTiles tt = term_tiles<R, V>(c, h.n, tpr, ref ? ref_ld / V : 0);
   const bool want = partials_out != nullptr;
   if (want) ensure_partials(c, (size_t)ld * 3 * tt.t[2].grid);
   int last_grid = 0;

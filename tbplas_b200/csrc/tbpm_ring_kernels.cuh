@@ -78,6 +78,7 @@ struct RingShape {
   int stages;       // S
   int cap;          // CSR entries a stage holds (multiple of 4)
   int pin_off, own_off, acc_off, diag_off, ip_off, ix_off, hop_off;
+  int ref_off;      // MODE 2: rows of the correlation reference (-1: read from global)
   int stage_bytes;  // one stage
   int bar_off;      // 2*S mbarriers (full[S], empty[S]) after the stages
   int smem_bytes;   // total dynamic shared memory
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
   const bool need_own = a.diag != nullptr || nflush >= 2;
   const bool add_acc = nflush > 0 && !a.c.acc_init;
   const int64_t row_bytes = (int64_t)tpr * sizeof(Pack<R, V>);
+  const bool ref_staged = MODE == 2 && a.ref != nullptr && sh.ref_off >= 0;
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -256,9 +258,11 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           bytes += d_bytes;
         }
         const uint32_t tile = (uint32_t)(nr * row_bytes);
+        const uint32_t ref_tile = (uint32_t)(nr * a.ref_tpr * (int64_t)sizeof(Pack<R, V>));
         if (a.pin) bytes += tile;
         if (need_own) bytes += tile;
         if (add_acc) bytes += tile;
+        if (ref_staged) bytes += ref_tile;
         ring_arrive_tx(bar, bytes);
         ring_copy(ring_smem(st + sh.ip_off), a.indptr + r0a, ip_bytes, bar);
         if (csr_in) {
@@ -277,6 +281,8 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           if (add_acc) ring_copy(ring_smem(st + sh.acc_off), a.acc + e0, tile, bar);
         }
         if (need_own) ring_copy(ring_smem(st + sh.own_off), a.gather + e0, tile, bar);
+        if (ref_staged)
+          ring_copy(ring_smem(st + sh.ref_off), a.ref + r0 * a.ref_tpr, ref_tile, bar);
       }
       __syncwarp();
       ++issued;
@@ -412,7 +418,11 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           stcs_pack(a.acc + e, acc);
           if (do_corr) {
             Pack<R, V> rf;
-            if (ref_lane) rf = ldcs_pack(a.ref + r * a.ref_tpr + lane);
+            if (ref_lane)
+              rf = ref_staged ? lds_pack<R, V>(st + sh.ref_off +
+                                               ((int64_t)slot * a.ref_tpr + lane) *
+                                                   sizeof(Pack<R, V>))
+                              : ldcs_pack(a.ref + r * a.ref_tpr + lane);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
               const double xr = (double)acc.v[2 * v], xi = (double)acc.v[2 * v + 1];
