@@ -216,3 +216,38 @@ def test_ring_kernel_with_a_dense_row(graphene_small):
     got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 12, 128, 1e-9)
     ref = oracle.tbpm_dos(bes, ip, ix, hv, 12, wf0=wf0)
     assert rel_err(got, ref) < FP64_TOL
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+@pytest.mark.parametrize("case", ["dimer", "chain5", "diagonal_only", "one_row"])
+def test_tiny_and_degenerate_hamiltonians(prec, tol, case):
+    """Fewer rows than one tile of the ring kernel (60 rows at 16 states), row
+    counts that are not multiples of 4 (the widened indptr window), no
+    off-diagonal entries at all (no CSR slice to stage), and a single row."""
+    if case == "dimer":
+        n, rows = 2, {0: [(1, -0.4)], 1: [(0, -0.4)]}
+    elif case == "chain5":
+        n = 5  # Hermitian: H[r][r+1] = -0.3 + 0.05i, H[r+1][r] its conjugate
+        rows = {r: [(c, -0.3 + 0.05j if c > r else -0.3 - 0.05j)
+                    for c in (r - 1, r + 1) if 0 <= c < n] for r in range(n)}
+        rows[2].append((2, 0.1))
+    elif case == "diagonal_only":
+        n = 7
+        rows = {r: [(r, 0.05 * (r - 3))] for r in range(n)}
+    else:
+        n, rows = 1, {0: [(0, 0.3)]}
+    ip = np.zeros(n + 1, dtype=np.int32)
+    ix, hv = [], []
+    for r in range(n):
+        ent = sorted(rows.get(r, []), key=lambda e: e[0])
+        ip[r + 1] = ip[r] + len(ent)
+        ix += [c for c, _ in ent]
+        hv += [v for _, v in ent]
+    ix = np.array(ix, dtype=np.int32)
+    hv = np.array(hv, dtype=np.complex128)
+    wf0 = unit_states(16, n, seed=3)
+    bes = bessel_series(math.pi)
+    f2py.set_backend(precision=prec)
+    got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 20, 8, 1e-9)
+    ref = oracle.tbpm_dos(bes, ip, ix, hv, 20, wf0=wf0)
+    assert rel_err(got, ref) < tol
