@@ -523,25 +523,47 @@ __global__ void __launch_bounds__(512) jcorr_kernel(
        r += (int64_t)gridDim.x * rpp) {
     R xxr = 0, xxi = 0, yxr = 0, yxi = 0, xyr = 0, xyi = 0, yyr = 0, yyi = 0;
     const int j0 = __ldg(indptr + r), j1 = __ldg(indptr + r + 1);
-    for (int j = j0; j < j1; ++j) {
-      const int c = __ldg(indices + j);
-      const typename Cx<R>::t h = ldg_c(hop + j);
-      const R jr = -s * h.y, ji = s * h.x;
-      const R ddx = __ldg(dx + j), ddy = __ldg(dy + j);
-      const typename Cx<R>::t p1x = ldg_c(psi + (int64_t)c * ld + b);
-      const typename Cx<R>::t p1y = ldg_c(psi + (int64_t)c * ld + B + b);
-      const R axr = jr * ddx, axi = ji * ddx, ayr = jr * ddy, ayi = ji * ddy;
-      // J_x psi1_x, J_y psi1_x, J_x psi1_y, J_y psi1_y
-      xxr = fma(axr, p1x.x, fma(-axi, p1x.y, xxr));
-      xxi = fma(axr, p1x.y, fma(axi, p1x.x, xxi));
-      yxr = fma(ayr, p1x.x, fma(-ayi, p1x.y, yxr));
-      yxi = fma(ayr, p1x.y, fma(ayi, p1x.x, yxi));
-      xyr = fma(axr, p1y.x, fma(-axi, p1y.y, xyr));
-      xyi = fma(axr, p1y.y, fma(axi, p1y.x, xyi));
-      yyr = fma(ayr, p1y.x, fma(-ayi, p1y.y, yyr));
-      yyi = fma(ayr, p1y.y, fma(ayi, p1y.x, yyi));
-    }
     const typename Cx<R>::t p2 = ldg_c(psi + r * ld + 2 * B + b);
+    // neighbours in batches of JB: every load of a batch is issued before the
+    // first product, so the gathers overlap (the products keep the entry order)
+    constexpr int JB = 4;
+    for (int jb = j0; jb < j1; jb += JB) {
+      int cc[JB];
+      typename Cx<R>::t hh[JB];
+      R ddx[JB], ddy[JB];
+#pragma unroll
+      for (int u = 0; u < JB; ++u) {
+        cc[u] = -1;
+        if (jb + u < j1) {
+          cc[u] = __ldg(indices + jb + u);
+          hh[u] = ldg_c(hop + jb + u);
+          ddx[u] = __ldg(dx + jb + u);
+          ddy[u] = __ldg(dy + jb + u);
+        }
+      }
+      typename Cx<R>::t p1x[JB], p1y[JB];
+#pragma unroll
+      for (int u = 0; u < JB; ++u)
+        if (cc[u] >= 0) {
+          p1x[u] = ldg_c(psi + (int64_t)cc[u] * ld + b);
+          p1y[u] = ldg_c(psi + (int64_t)cc[u] * ld + B + b);
+        }
+#pragma unroll
+      for (int u = 0; u < JB; ++u) {
+        if (cc[u] < 0) continue;
+        const R jr = -s * hh[u].y, ji = s * hh[u].x;
+        const R axr = jr * ddx[u], axi = ji * ddx[u], ayr = jr * ddy[u], ayi = ji * ddy[u];
+        // J_x psi1_x, J_y psi1_x, J_x psi1_y, J_y psi1_y
+        xxr = fma(axr, p1x[u].x, fma(-axi, p1x[u].y, xxr));
+        xxi = fma(axr, p1x[u].y, fma(axi, p1x[u].x, xxi));
+        yxr = fma(ayr, p1x[u].x, fma(-ayi, p1x[u].y, yxr));
+        yxi = fma(ayr, p1x[u].y, fma(ayi, p1x[u].x, yxi));
+        xyr = fma(axr, p1y[u].x, fma(-axi, p1y[u].y, xyr));
+        xyi = fma(axr, p1y[u].y, fma(axi, p1y[u].x, xyi));
+        yyr = fma(ayr, p1y[u].x, fma(-ayi, p1y[u].y, yyr));
+        yyi = fma(ayr, p1y[u].y, fma(ayi, p1y[u].x, yyi));
+      }
+    }
     const double qr = (double)p2.x, qi = (double)p2.y;
     // conj(p2) * v
     acc[0] += qr * (double)xxr + qi * (double)xxi;
