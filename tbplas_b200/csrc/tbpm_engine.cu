@@ -1466,7 +1466,7 @@ void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double 
   C* P = c->X.as<C>();
   C* ring = c->Y.as<C>();  // 5 vectors: T ring (3) and the P carry (2)
   C* psi = c->wf0.as<C>();
-  double2* ws = c->qe.as<double2>();  // split partials of the contraction
+  double2* ws = nullptr;  // split partials of the contraction (c->qe)
   const int grid = (int)std::min<int64_t>(blocks_for(n, 256), (int64_t)kSMs * 16);
   const C* diag = h.has_diag ? h.diag.as<C>() : nullptr;
   const R* dj = direction == 1 ? h.dx.as<R>() : h.dy.as<R>();
@@ -1511,6 +1511,9 @@ void kbdc_state(tbpm_ctx* c, int nk, int direction, const double* g_dev, double 
         hmv(2.0, -1.0, pm1, pm2, pi);  // p_i = 2 H p_i-1 - p_i-2 (:950)
     }
     const PqSplit sp = pq_split(c, n, m, nk);
+    // a short last chunk may take more slices than the full chunks it was sized for
+    c->qe.ensure((size_t)sp.slices * m * nk * sizeof(double2));
+    ws = c->qe.as<double2>();
     pq_gemm_kernel<R><<<dim3((nk + kPqTile - 1) / kPqTile, (m + kPqTile - 1) / kPqTile,
                              sp.slices),
                         256, 0, c->stream>>>(P, Q, n, m, nk, sp.rows, ws);
