@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <optional>
 #include <type_traits>
 
 #include "tbpm_engine.cuh"
@@ -24,7 +25,6 @@
 #include "tbpm_kernels.cuh"
 #include "tbpm_ring_kernels.cuh"
 #include "tbpm_pq_gemm.cuh"
-#include "tbpm_ring_kernels.cuh"
 #include "tbpm_more_kernels.cuh"
 #include "tbpm_scan.cuh"
 
@@ -1150,6 +1150,8 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   std::vector<double> host;
   const double pi = 3.14159265358979323846;
   // ---- phase 1: +/- dt propagation, DOS correlation, QE accumulation ----
+  std::optional<Phase> phase;
+  phase.emplace("tbpm_dccond: quasi-eigenstates");
   int t = 1;
   bool first_window = true;
   while (t <= n_timestep) {
@@ -1252,6 +1254,7 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       }
   if (n_en == 0) return;
   // ---- phase 2 ----
+  phase.emplace("tbpm_dccond: current correlations");
   const int n_ib = n_en * nb;
   int64_t rows_per_tile = std::max<int64_t>(64, n / ((int64_t)kSMs * 8));
   const int pgrid = (int)((n + rows_per_tile - 1) / rows_per_tile);
@@ -1893,6 +1896,7 @@ void ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices, cons
 void drv_ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
                     const double* hop, int64_t n, int64_t nnz, const double* dx,
                     const double* dy, double rescale) {
+  Phase phase("tbpm_ham_upload");
   if (!indptr || (nnz > 0 && (!indices || !hop))) throw Error{TBPM_ERR_ARG, "null CSR array"};
   ham_upload(c, indptr, indices, hop, n, nnz, dx, dy, rescale);
 }
@@ -1900,6 +1904,7 @@ void drv_ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices,
 void drv_dos(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, int n_states,
              int seed, int rank, int n_ran_samples, int n_timestep, int chk_step,
              double chk_thr, double* corr, double* corr_per_state) {
+  Phase phase("tbpm_dos");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
@@ -1931,6 +1936,7 @@ void drv_ac(tbpm_ctx* c, const double* bes, int n_bes, double beta, double mu,
             const double* wf0, int n_states, int seed, int rank, int n_ran_samples,
             int n_timestep, int nr_fermi, double fermi_precision, int chk_step, double chk_thr,
             double* corr) {
+  Phase phase("tbpm_accond");
   require_ham(c, true);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
@@ -1975,6 +1981,7 @@ void drv_dc_part(tbpm_ctx* c, const double* bes, int n_bes, const double* wf0, i
                  double t_step, const double* energies, int n_energies, const int32_t* en_inds,
                  int n_en_inds, int chk_step, double chk_thr, double* dos_corr, double* dc_corr,
                  bool zero) {
+  Phase phase("tbpm_dccond");
   require_ham(c, true);
   if (first_state < 0 || n_avg < 1) throw Error{TBPM_ERR_ARG, "bad state range"};
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
@@ -2073,6 +2080,7 @@ void drv_dyn_pol(tbpm_ctx* c, const double* bes, int n_bes, double beta, double 
                  int n_q, const double* wf0, int n_states, int seed, int rank,
                  int n_ran_samples, int n_timestep, int nr_fermi, double fermi_precision,
                  int chk_step, double chk_thr, double* corr) {
+  Phase phase("tbpm_dyn_pol");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
@@ -2130,6 +2138,7 @@ void drv_eigenstates(tbpm_ctx* c, const double* bes, int n_bes, const double* wf
                      int n_states, int seed, int rank, int n_ran_samples, int n_timestep,
                      double t_step, const double* energies, int n_energies, int chk_step,
                      double chk_thr, double* wf_qe) {
+  Phase phase("tbpm_eigenstates");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
@@ -2183,6 +2192,7 @@ void drv_eigenstates(tbpm_ctx* c, const double* bes, int n_bes, const double* wf
 
 void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
               int n_ran_samples, int n_kernel, int direction, double* mu) {
+  Phase phase("tbpm_kbdc");
   require_ham(c, true);
   if (n_states < 1) throw Error{TBPM_ERR_ARG, "n_ran_samples must be >= 1"};
   if (n_kernel < 2) throw Error{TBPM_ERR_ARG, "n_kernel must be >= 2"};
@@ -2246,6 +2256,7 @@ void drv_kbdc(tbpm_ctx* c, const double* wf0, int n_states, int seed, int rank,
 
 void drv_haydock(tbpm_ctx* c, const int32_t* sites, int n_sites, const double* wf_sites,
                  int n_samples, int n_depth, double h_rescale, double* coefa, double* coefb) {
+  Phase phase("tbpm_haydock");
   require_ham(c, false);
   if (!sites || n_sites < 1 || !wf_sites || n_samples < 1)
     throw Error{TBPM_ERR_ARG, "site indices and site amplitudes required"};
@@ -2347,6 +2358,7 @@ void drv_cond_from_trace(tbpm_ctx* c, const double* mu_mn, int nk, const double*
 void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t* seg_off,
                        int n_seg, int n_states, int seed, int n_timestep, int chk_step,
                        double chk_thr, double* corr, double* corr_per_state) {
+  Phase phase("tbpm_dos_segmented");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_timestep < 1) throw Error{TBPM_ERR_ARG, "n_timestep must be >= 1"};
@@ -2372,6 +2384,7 @@ void drv_dos_segmented(tbpm_ctx* c, const double* bes, int n_bes, const int64_t*
 void drv_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const double* psi0,
                const int32_t* time_log, int n_log, int n_timestep, int chk_step,
                double chk_thr, double* psi_t) {
+  Phase phase("tbpm_psi_t");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_log < 1 || !time_log) throw Error{TBPM_ERR_ARG, "time_log must not be empty"};
@@ -2392,6 +2405,7 @@ void drv_psi_t(tbpm_ctx* c, const double* bes, int n_bes, const double* psi0,
 
 void drv_random_states(tbpm_ctx* c, int64_t n, int seed, int first_sample, int n_states,
                        int rank, int n_ran_samples, int kind, double* wf) {
+  Phase phase("tbpm_random_states");
   if (n < 1 || n_states < 1) throw Error{TBPM_ERR_ARG, "bad sizes"};
   c->sess.active = false;
   c->graph.reset();
@@ -2428,6 +2442,7 @@ void drv_fermi_coef(int nr_fermi, double beta, double mu, int one_minus, double 
 }
 
 void drv_expansion_apply(tbpm_ctx* c, const Expansion& ex, double* wf, int n_states) {
+  Phase phase("tbpm_expansion_apply");
   require_ham(c, false);
   if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
   c->graph.reset();
@@ -2446,6 +2461,7 @@ void drv_expansion_apply(tbpm_ctx* c, const Expansion& ex, double* wf, int n_sta
 
 void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_states, int seed,
                            int rank, int n_ran_samples, int n_timestep) {
+  Phase phase("tbpm_session_dos_begin");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};
@@ -2462,6 +2478,7 @@ void drv_session_dos_begin(tbpm_ctx* c, const double* bes, int n_bes, int n_stat
 }
 
 void drv_session_advance(tbpm_ctx* c, int n_steps) {
+  Phase phase("tbpm_session_advance");
   if (!c->sess.active) throw Error{TBPM_ERR_STATE, "no session active"};
   if (n_steps < 0) throw Error{TBPM_ERR_ARG, "n_steps < 0"};
   dispatch(c->ham.prec, c->sess.V, [&](auto tag) {
@@ -2473,6 +2490,7 @@ void drv_session_advance(tbpm_ctx* c, int n_steps) {
 void drv_session_dos_resume(tbpm_ctx* c, const double* bes, int n_bes, int n_states,
                             const double* wf0, const double* psi, const double* corr,
                             const double* norms, int n_done, int n_timestep) {
+  Phase phase("tbpm_session_dos_resume");
   require_ham(c, false);
   if (!bes || n_bes < 3) throw Error{TBPM_ERR_ARG, "at least 3 Bessel coefficients required"};
   if (n_states < 1 || n_states > kMaxCols) throw Error{TBPM_ERR_ARG, "1..64 states"};

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <mutex>
@@ -24,6 +25,16 @@ void throw_cuda(cudaError_t e, const char* what);
     cudaError_t e_ = (call);                            \
     if (e_ != cudaSuccess) ::tbpm::throw_cuda(e_, #call); \
   } while (0)
+
+// A named NVTX range over a scope (a driver or one of its phases), so that a
+// timeline profiler shows where each call spends its time. NVTX3 is header
+// only: with no profiler attached each push/pop is a test of a null pointer.
+struct Phase {
+  explicit Phase(const char* name) { nvtxRangePushA(name); }
+  ~Phase() { nvtxRangePop(); }
+  Phase(const Phase&) = delete;
+  Phase& operator=(const Phase&) = delete;
+};
 
 // Grow-only device allocation, in multiples of 256 bytes (the bulk copies of
 // the ring kernels widen their windows to 16-byte boundaries and rely on it).

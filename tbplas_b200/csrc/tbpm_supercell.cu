@@ -701,6 +701,7 @@ void fill_split(const Prepared& P, const int64_t* off, Ham& h, bool dxy, bool di
 // (in place of tbpm_ham_upload of a host CSR).
 void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
                        int64_t* n_rows, int64_t* nnz, double* rescale) {
+  Phase phase("tbpm_supercell_ham");
   Prepared P;
   prepare(c, sc, layout, cutoff, P);
   const bool dxy = layout == TBPM_LAYOUT_DXY;
@@ -756,6 +757,7 @@ void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double
 void drv_supercell_csr(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double cutoff,
                        int64_t* n_rows, int64_t* nnz, double* rescale, int64_t* indptr,
                        int32_t* indices, double* hop, double* dx, double* dy) {
+  Phase phase("tbpm_supercell_csr");
   Prepared P;
   prepare(c, sc, layout, cutoff, P);
   const bool dxy = layout == TBPM_LAYOUT_DXY;
