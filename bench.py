@@ -144,7 +144,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes):
+def algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes, paired=False, with_ref=True):
     """HBM bytes one time step of the fused kernel family must move.
 
     Per Chebyshev term k = 1..n_bes-1 the kernel reads the CSR once
@@ -152,16 +152,21 @@ def algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes):
     (neighbour rows come from L2), reads p_{k-2} and writes p_k (not on the
     first and last term), and every third term flushes the accumulator
     (read + write; write only on the first flush); the last term also reads
-    the correlation reference.  This mirrors the kernel schedule of
-    tbplas_b200/csrc/tbpm_engine.cu (enqueue_expansion).
+    the correlation reference (with_ref).  With paired terms (two terms per
+    launch) the second term of a pair reads p_k, its own rows of p_{k-1} and
+    the CSR from L2: the pair saves the CSR and two vector passes.  Pairs are
+    (1, 2), (3, 4), ... except a last term with the correlation and two flush
+    terms in a row.  This mirrors the schedule of enqueue_expansion in
+    tbplas_b200/csrc/tbpm_engine.cu.
     """
     sv = 2 * real_bytes
     vec = n * ld * sv
     mat = (n + 1) * 4 + nnz * (4 + sv)
-    total = 0.0
+    term, flush = {}, {}
     last_flush = -1
     for k in range(1, n_bes):
         b = mat + vec
+        fl = False
         if k == 1:
             b += vec
         else:
@@ -170,9 +175,20 @@ def algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes):
             if k == 2 or pending == 3 or k == n_bes - 1:
                 b += vec * (1 if k == 2 else 2)
                 last_flush = k
-        if k == n_bes - 1:
+                fl = True
+        if k == n_bes - 1 and with_ref:
             b += vec  # correlation reference wf0
-        total += b
+        term[k], flush[k] = b, fl
+    total = 0.0
+    k = 1
+    while k < n_bes:
+        if (paired and k + 1 < n_bes and not (with_ref and k + 1 == n_bes - 1)
+                and not (flush[k] and flush[k + 1])):
+            total += term[k] + term[k + 1] - mat - 2 * vec
+            k += 2
+        else:
+            total += term[k]
+            k += 1
     return total
 
 
@@ -183,14 +199,15 @@ def survey_model_bytes_per_orbital_step(n, nnz, ld, n_bes, real_bytes):
     return ((n_bes - 1) * (m / (n * ld) + 5 * sv) + sv)
 
 
-def ac_algorithmic_bytes_per_step(n, nnz, nb, n_bes, real_bytes):
+def ac_algorithmic_bytes_per_step(n, nnz, nb, n_bes, real_bytes, paired=False):
     """HBM bytes of one AC time step: the time-step expansion of the
     3*nb-column block (no correlation reference on its last term) plus the
     current-correlation pass, which reads the CSR with hop, dx and dy once
     and every column of the block once."""
     ld = 3 * nb
     sv = 2 * real_bytes
-    exp = algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes) - n * ld * sv
+    exp = algorithmic_bytes_per_step(n, nnz, ld, n_bes, real_bytes, paired=paired,
+                                     with_ref=False)
     jcorr = (n + 1) * 4 + nnz * (4 + sv + 2 * real_bytes) + n * ld * sv
     return exp + jcorr
 
@@ -250,7 +267,7 @@ def parity_spot_check(ip, ix, hv, bes, corr_rows, rank, columns=(0, 1), steps=2)
     return worst
 
 
-def time_ac(args, sample, rank, local, peak):
+def time_ac(args, sample, rank, local, peak, paired):
     """Device time per AC time step (FP64, 16 states, 48-column block)."""
     import torch
     from tbplas_b200 import KB
@@ -287,7 +304,7 @@ def time_ac(args, sample, rank, local, peak):
     t1 = run(short)
     t2 = run(short + extra)
     ms = (t2 - t1) / extra
-    alg = ac_algorithmic_bytes_per_step(n, nnz, N_STATES, bes.size, 8)
+    alg = ac_algorithmic_bytes_per_step(n, nnz, N_STATES, bes.size, 8, paired=paired)
     gbs = alg / (ms * 1e-3) / 1e9
     return {"ms_per_step": ms, "orbital_steps_per_s": n * N_STATES / (ms * 1e-3),
             "alg_bytes_per_step": alg, "achieved_gbs": gbs, "roofline_frac": gbs / peak,
@@ -368,7 +385,12 @@ def run_gpu(args):
         launches = (l1 - l0)
         model_bytes_step = (b1 - b0) / args.steps
         rb = 8 if prec == nat.PREC_FP64 else 4
-        alg = algorithmic_bytes_per_step(n, nnz, N_STATES, n_bes, rb)
+        # the library ran two terms per launch where its byte count matches
+        # the paired schedule
+        alg_single = algorithmic_bytes_per_step(n, nnz, N_STATES, n_bes, rb)
+        alg_paired = algorithmic_bytes_per_step(n, nnz, N_STATES, n_bes, rb, paired=True)
+        paired = abs(model_bytes_step - alg_paired) < abs(model_bytes_step - alg_single)
+        alg = alg_paired if paired else alg_single
         corr = np.zeros((total + 1, N_STATES), dtype=np.complex128)
         norms = np.zeros((total + 1, N_STATES))
         import ctypes
@@ -382,6 +404,8 @@ def run_gpu(args):
             "orbital_steps_per_s": n * N_STATES * world / (ms_step * 1e-3),
             "launches": launches,
             "alg_bytes_per_step": alg,
+            "alg_bytes_per_step_single_terms": alg_single,
+            "paired_terms": bool(paired),
             "lib_model_bytes_per_step": model_bytes_step,
             "achieved_gbs": alg / (ms_step * 1e-3) / 1e9,
             "norm_drift": float(np.max(np.abs(norms[:nd.value] - norms[0]))),
@@ -420,7 +444,7 @@ def run_gpu(args):
     # ---- AC time step of the same workload (FP64) -------------------------
     ac = None
     if not args.skip_ac:
-        ac = time_ac(args, sample, rank, local, peak)
+        ac = time_ac(args, sample, rank, local, peak, results["fp64"]["paired_terms"])
         if distributed:
             ac_ms, ac_ranks = gather_rank_values(ac["ms_per_step"], dist, dev)
             ac["ms_per_step"] = ac_ms
@@ -480,7 +504,8 @@ def run_gpu(args):
                                 "the 1024x1024 case, scaled by rows to this workload",
                 "alg_bytes_per_step": r64["alg_bytes_per_step"],
                 "kernel": ("cheb_term_kernel<double,2,MODE>" if args.term_kernel == 1 else
-                           "cheb_ring_kernel<double,2,MODE>") +
+                           "cheb_pair_kernel<double,2> + cheb_ring_kernel<double,2,2>"
+                           if r64["paired_terms"] else "cheb_ring_kernel<double,2,MODE>") +
                           " (+ finalize_kernel, <1% of step)",
             },
             "e2e": e2e,
@@ -609,9 +634,11 @@ def main():
     ap.add_argument("--vector-width", type=int, default=0, choices=[0, 1, 2],
                     help="FP64 complex values per thread: 0 library default (two, 256-bit "
                          "accesses), 1 one (128-bit accesses), 2 two")
-    ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2],
-                    help="Chebyshev-term kernel: 0 library default (shared-memory ring fed by "
-                         "bulk copies), 1 grid-stride kernel with plain loads, 2 ring")
+    ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="Chebyshev-term kernel: 0 library default (two terms per launch "
+                         "where the dependency lists allow, else the shared-memory ring), "
+                         "1 grid-stride kernel with plain loads, 2 ring (one term per "
+                         "launch), 3 two terms per launch wherever the lists fit")
     ap.add_argument("--threads", type=int, default=0,
                     help="FP64 threads per block of the term kernel (0: library default)")
     ap.add_argument("--nx", type=int, default=2048,

@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libtbpm_b200.so")
 SOURCES = ["tbpm_engine.cu", "tbpm_capi.cu", "tbpm_noalloc.cu", "tbpm_nn.cu",
            "tbpm_supercell.cu", "tbpm_nn_tc.cu", "tbpm_analysis.cu"]
 HEADERS = ["tbpm_common.cuh", "tbpm_kernels.cuh", "tbpm_ring_kernels.cuh", "tbpm_pq_gemm.cuh",
+           "tbpm_pair_kernels.cuh",
            "tbpm_dc_kernels.cuh",
            "tbpm_seg_kernels.cuh",
            "tbpm_more_kernels.cuh", "tbpm_scan.cuh",

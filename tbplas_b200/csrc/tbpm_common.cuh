@@ -139,6 +139,73 @@ __device__ __forceinline__ void stcs_pack(Pack<float, 1>* p, const Pack<float, 1
 __device__ __forceinline__ double2 ldg_c(const double2* p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldg_c(const float2* p) { return __ldg(p); }
 
+// Loads of values written earlier in the same launch by other blocks: cached
+// in L2 only (ld.global.cg), never in the non-coherent L1/texture path.  The
+// asm statements are volatile with a memory clobber so the compiler keeps
+// them after the synchronisation that makes the values visible.
+__device__ __forceinline__ Pack<double, 1> ldcg_pack(const Pack<double, 1>* p) {
+  Pack<double, 1> r;
+  asm volatile("ld.global.cg.v2.f64 {%0, %1}, [%2];" : "=d"(r.v[0]), "=d"(r.v[1]) : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ Pack<double, 2> ldcg_pack(const Pack<double, 2>* p) {
+  Pack<double, 2> r;
+  asm volatile("ld.global.cg.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ Pack<float, 1> ldcg_pack(const Pack<float, 1>* p) {
+  Pack<float, 1> r;
+  asm volatile("ld.global.cg.v2.f32 {%0, %1}, [%2];" : "=f"(r.v[0]), "=f"(r.v[1]) : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ Pack<float, 2> ldcg_pack(const Pack<float, 2>* p) {
+  Pack<float, 2> r;
+  asm volatile("ld.global.cg.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+__device__ __forceinline__ Pack<float, 4> ldcg_pack(const Pack<float, 4>* p) {
+  Pack<float, 4> r;
+  asm volatile("ld.global.cg.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]),
+                 "=f"(r.v[5]), "=f"(r.v[6]), "=f"(r.v[7])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+
+// Stores with the default (write-back, evict-normal) policy, for values that
+// are read again from L2 shortly after, within the same launch.
+__device__ __forceinline__ void stwb_pack(Pack<double, 1>* p, const Pack<double, 1>& v) {
+  asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v.v[0]), "d"(v.v[1]) : "memory");
+}
+__device__ __forceinline__ void stwb_pack(Pack<double, 2>* p, const Pack<double, 2>& v) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(v.v[0]), "d"(v.v[1]),
+               "d"(v.v[2]), "d"(v.v[3])
+               : "memory");
+}
+__device__ __forceinline__ void stwb_pack(Pack<float, 1>* p, const Pack<float, 1>& v) {
+  asm volatile("st.global.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v.v[0]), "f"(v.v[1]) : "memory");
+}
+__device__ __forceinline__ void stwb_pack(Pack<float, 2>* p, const Pack<float, 2>& v) {
+  asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.v[0]), "f"(v.v[1]),
+               "f"(v.v[2]), "f"(v.v[3])
+               : "memory");
+}
+__device__ __forceinline__ void stwb_pack(Pack<float, 4>* p, const Pack<float, 4>& v) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p),
+               "f"(v.v[0]), "f"(v.v[1]), "f"(v.v[2]), "f"(v.v[3]), "f"(v.v[4]), "f"(v.v[5]),
+               "f"(v.v[6]), "f"(v.v[7])
+               : "memory");
+}
+
 // Fixed-order tree reduction over the `rows` row slots of a block.  Values are
 // laid out as smem[slot * width + k]; after the call slot 0 holds the sums.
 // Every thread of the block must call it (it synchronises).

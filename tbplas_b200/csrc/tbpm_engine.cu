@@ -25,6 +25,7 @@
 #include "tbpm_kernels.cuh"
 #include "tbpm_ring_kernels.cuh"
 #include "tbpm_pq_gemm.cuh"
+#include "tbpm_pair_kernels.cuh"
 #include "tbpm_more_kernels.cuh"
 #include "tbpm_scan.cuh"
 
@@ -391,6 +392,130 @@ int launch_term(tbpm_ctx* c, const TermTiles& tt, const TermArgs<R, V>& a) {
   return t.grid;
 }
 
+// ---- paired terms (tbpm_pair_kernels.cuh) --------------------------------
+
+template <typename R, int V>
+int pair_blocks_per_sm(const tbpm_ctx* c, size_t smem) {
+  static bool attr_set[64] = {false};
+  const int dev = c->device;
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    TBPM_CK(cudaFuncSetAttribute(cheb_pair_kernel<R, V>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr_set[dev] = true;
+  }
+  return resident_per_sm(cheb_pair_kernel<R, V>, kRingThreads, smem);
+}
+
+// L2 the rows between a tile's two terms may occupy: the second term finds
+// p_k, p_{k-1} and the CSR slice of its tile in L2 while the tiles started
+// in between (the margin plus the dependency lag) fit in this budget.
+constexpr size_t kPairL2Window = 48ull << 20;
+
+// Build the plan for tiles of `rows` rows on the device: dependency lists
+// (pair_fwd/rev/merge_kernel), the item sequence (pair_seq_kernel), zeroed
+// flags and counters.  usable: every list fits kPairDeps and, unless forced,
+// at least 90% of the tiles have their last dependency within the L2 window.
+void build_pair_plan(tbpm_ctx* c, PairPlan& p, const PairRequest& q) {
+  const Ham& h = c->ham;
+  cudaStream_t st = c->stream;
+  const int TR = q.rows;
+  const int64_t nt64 = (h.n + TR - 1) / TR;
+  if (nt64 < 1 || nt64 > (1 << 29)) throw Error{TBPM_ERR_ARG, "too many row tiles to pair"};
+  const int nt = (int)nt64;
+  p.rows = TR;
+  p.grid = q.grid;
+  p.ham_gen = h.gen;
+  p.forced = q.force;
+  p.usable = false;
+  p.n_tiles = nt;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_list = al((size_t)nt * kPairDeps * 4), b_t = al((size_t)nt * 4),
+               b_t1 = al((size_t)(nt + 1) * 4), b_off = al((size_t)(nt + 2) * 8);
+  c->pair_tmp.ensure(2 * b_list + 3 * b_t + 2 * b_t1 + b_off + 256);
+  char* w = c->pair_tmp.as<char>();
+  int* fwd = reinterpret_cast<int*>(w);
+  int* rev = reinterpret_cast<int*>(w += b_list);
+  int* fcnt = reinterpret_cast<int*>(w += b_list);
+  int* rcnt = reinterpret_cast<int*>(w += b_t);
+  int* ready = reinterpret_cast<int*>(w += b_t);
+  int* cnt_b = reinterpret_cast<int*>(w += b_t);
+  int* g_cnt = reinterpret_cast<int*>(w += b_t1);
+  int64_t* off_b = reinterpret_cast<int64_t*>(w += b_t1);
+  unsigned* flags2 = reinterpret_cast<unsigned*>(w += b_off);  // [0] bad, [1] near
+  p.seq.ensure((size_t)2 * nt * sizeof(int4));
+  p.deps.ensure((size_t)nt * kPairDeps * 4);
+  p.flags.ensure((size_t)nt * 4);
+  p.sync.ensure(sizeof(PairSync));
+  TBPM_CK(cudaMemsetAsync(rcnt, 0, (size_t)nt * 4, st));
+  TBPM_CK(cudaMemsetAsync(cnt_b, 0, (size_t)(nt + 1) * 4, st));
+  TBPM_CK(cudaMemsetAsync(g_cnt, 0, (size_t)(nt + 1) * 4, st));
+  TBPM_CK(cudaMemsetAsync(flags2, 0, 8, st));
+  TBPM_CK(cudaMemsetAsync(p.flags.p, 0, (size_t)nt * 4, st));
+  TBPM_CK(cudaMemsetAsync(p.sync.p, 0, sizeof(PairSync), st));
+  const int margin = q.grid * (q.stages + kPairBatch) / 2;
+  const long long window = (long long)(kPairL2Window / std::max<size_t>(3 * q.tile_bytes, 1));
+  const int near = (int)std::max<long long>(0, std::min<long long>(window - margin, nt));
+  const int gw = (int)std::min<int64_t>((nt + 7) / 8, (int64_t)kSMs * 16);
+  const int gt = (int)std::min<int64_t>(blocks_for(nt, 256), (int64_t)kSMs * 16);
+  pair_fwd_kernel<<<gw, 256, 0, st>>>(h.indptr.as<int32_t>(), h.indices.as<int32_t>(), h.n, TR,
+                                      nt, fwd, fcnt, flags2);
+  pair_rev_kernel<<<gt, 256, 0, st>>>(fwd, fcnt, nt, rev, rcnt, flags2);
+  pair_merge_kernel<<<gt, 256, 0, st>>>(fwd, fcnt, rev, rcnt, nt, margin, near,
+                                        p.deps.as<int>(), ready, cnt_b, flags2, flags2 + 1);
+  TBPM_CK(cudaGetLastError());
+  scan_counts(cnt_b, nt + 1, off_b, st);
+  pair_seq_kernel<<<gt, 256, 0, st>>>(h.indptr.as<int32_t>(), h.n, TR, nt, ready, off_b, g_cnt,
+                                      p.seq.as<int4>());
+  TBPM_CK(cudaGetLastError());
+  unsigned host[2] = {0, 0};
+  TBPM_CK(cudaMemcpyAsync(host, flags2, 8, cudaMemcpyDeviceToHost, st));
+  TBPM_CK(cudaStreamSynchronize(st));
+  p.usable = host[0] == 0 && (q.force || (double)host[1] >= 0.9 * (double)nt);
+}
+
+// The plan for tiles of q.rows rows on the current Hamiltonian, built when
+// missing or stale; null when pairs do not apply.  During a graph capture a
+// missing plan is recorded in c->pair_requests instead (ensure_graph builds it
+// and captures again) and this call returns null.
+PairPlan* pair_plan(tbpm_ctx* c, const PairRequest& q) {
+  PairPlan* p = nullptr;
+  for (auto& e : c->pairs)
+    if (e->rows == q.rows) p = e.get();
+  if (p && p->ham_gen == c->ham.gen && p->grid == q.grid && p->forced == q.force)
+    return p->usable ? p : nullptr;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TBPM_CK(cudaStreamIsCapturing(c->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    c->pair_requests.push_back(q);
+    return nullptr;
+  }
+  if (!p) {
+    c->pairs.push_back(std::make_unique<PairPlan>());
+    p = c->pairs.back().get();
+  }
+  build_pair_plan(c, *p, q);
+  return p->usable ? p : nullptr;
+}
+
+template <typename R, int V>
+void launch_pair(tbpm_ctx* c, const PairPlan& pp, const RingShape& rs, const TermArgs<R, V>& a0,
+                 const TermArgs<R, V>& a1) {
+  PairArgs<R, V> pa;
+  pa.t[0] = a0;
+  pa.t[1] = a1;
+  pa.s = rs;
+  pa.seq = pp.seq.as<int4>();
+  pa.n_items = 2 * pp.n_tiles;
+  pa.deps = pp.deps.as<int>();
+  pa.flags = pp.flags.as<unsigned>();
+  pa.sync = pp.sync.as<PairSync>();
+  pa.status = c->status.as<unsigned int>();
+  cheb_pair_kernel<R, V><<<pp.grid, kRingThreads, (size_t)rs.smem_bytes + kPairExtraSmem,
+                           c->stream>>>(pa);
+  TBPM_CK(cudaGetLastError());
+  c->launches++;
+}
+
 // Enqueue one expansion (one time step, or one Fermi operator) on the block A.
 // When `partials_out` is set the last term also produces <ref|psi>, <psi|psi>
 // block partials and a finalize launch stores them in out[*step].
@@ -413,8 +538,11 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
   const double vec = (double)h.n * ld * sv;
   const double mat = (double)(h.n + 1) * 4 + (double)h.nnz * (4 + 2 * sizeof(R)) +
                      (h.has_diag ? (double)h.n * 2 * sizeof(R) : 0.0);
+  std::vector<TermArgs<R, V>> terms(std::max(n, 1));
+  std::vector<double> term_bytes(std::max(n, 1), 0.0);
   for (int k = 1; k < n; ++k) {
-    TermArgs<R, V> a{};
+    TermArgs<R, V>& a = terms[k];
+    a = TermArgs<R, V>{};
     a.indptr = h.indptr.as<int32_t>();
     a.indices = h.indices.as<int32_t>();
     a.hop = h.hop.as<typename Cx<R>::t>();
@@ -463,8 +591,43 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
       a.partials = c->partials.as<double>();
       if (ref) bytes += (double)h.n * ref_ld * sv;
     }
-    last_grid = launch_term<R, V>(c, tt, a);
-    c->model_bytes += bytes;
+    term_bytes[k] = bytes;
+  }
+  // Terms k, k+1 run as one paired launch where the plan applies, except a
+  // last term with correlation partials and two flush terms in a row (the
+  // second would stage accumulator rows the first wrote in the same launch).
+  PairPlan* pp = nullptr;
+  RingShape prs{};
+  const int tk = c->opts.term_kernel;
+  if (n >= 3 && (tk == 0 || tk == 3) && tt.ring[1]) {
+    prs = tt.rs[1];
+    const size_t smem = (size_t)prs.smem_bytes + kPairExtraSmem;
+    if (smem <= 227 * 1024) {
+      const int per_sm = pair_blocks_per_sm<R, V>(c, smem);
+      const int64_t tiles = (h.n + prs.rows - 1) / prs.rows;
+      PairRequest q;
+      q.rows = prs.rows;
+      q.grid = (int)std::max<int64_t>(
+          1, std::min<int64_t>((int64_t)per_sm * num_sms(c->device), tiles));
+      q.stages = prs.stages;
+      q.tile_bytes = (size_t)prs.rows * tpr * sizeof(Pack<R, V>);
+      q.force = tk == 3;
+      pp = pair_plan(c, q);
+    }
+  }
+  for (int k = 1; k < n;) {
+    const bool pair = pp && k + 1 < n && !(want && k + 1 == n - 1) &&
+                      !(terms[k].c.nflush > 0 && terms[k + 1].c.nflush > 0);
+    if (pair) {
+      launch_pair<R, V>(c, *pp, prs, terms[k], terms[k + 1]);
+      // the second term reads p_k, its own p_{k-1} rows and the matrix from L2
+      c->model_bytes += term_bytes[k] + term_bytes[k + 1] - mat - 2 * vec;
+      k += 2;
+    } else {
+      last_grid = launch_term<R, V>(c, tt, terms[k]);
+      c->model_bytes += term_bytes[k];
+      k += 1;
+    }
   }
   if (want) launch_finalize(c, last_grid, ld * 3, k_ctr, partials_out);
 }
@@ -605,19 +768,34 @@ void ensure_graph(tbpm_ctx* c, const std::vector<unsigned char>& key, Fn&& step,
   c->graph.reset();
   const int64_t l0 = c->launches;
   const double b0 = c->model_bytes;
-  TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
-  try {
-    for (int i = 0; i < G; ++i) step();
-  } catch (...) {
-    cudaGraph_t g = nullptr;
-    cudaStreamEndCapture(c->stream, &g);
-    if (g) cudaGraphDestroy(g);
+  cudaGraph_t g = nullptr;
+  // a capture that asked for paired-term plans is discarded; the plans are
+  // built (outside the capture) and the steps captured again
+  for (int attempt = 0;; ++attempt) {
+    c->pair_requests.clear();
+    TBPM_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    try {
+      for (int i = 0; i < G; ++i) step();
+    } catch (...) {
+      cudaGraph_t gx = nullptr;
+      cudaStreamEndCapture(c->stream, &gx);
+      if (gx) cudaGraphDestroy(gx);
+      c->launches = l0;
+      c->model_bytes = b0;
+      c->pair_requests.clear();
+      throw;
+    }
+    TBPM_CK(cudaStreamEndCapture(c->stream, &g));
+    if (c->pair_requests.empty() || attempt > 0) break;
+    cudaGraphDestroy(g);
+    g = nullptr;
     c->launches = l0;
     c->model_bytes = b0;
-    throw;
+    const std::vector<PairRequest> reqs = c->pair_requests;
+    c->pair_requests.clear();
+    for (const PairRequest& q : reqs) pair_plan(c, q);
   }
-  cudaGraph_t g = nullptr;
-  TBPM_CK(cudaStreamEndCapture(c->stream, &g));
+  c->pair_requests.clear();
   cudaError_t e = cudaGraphInstantiate(&c->graph.exec, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) {
@@ -680,6 +858,8 @@ std::vector<unsigned char> plan_key(const tbpm_ctx* c, int kind, int ld, int V,
   key_push(k, c->ham.has_diag);
   key_push(k, c->ham.has_dxy);
   key_push(k, c->ham.rescale);
+  key_push(k, c->ham.gen);
+  key_push(k, c->opts.term_kernel);
   const void* ptrs[] = {c->ham.indptr.p, c->ham.indices.p, c->ham.hop.p,  c->ham.dx.p,
                         c->ham.dy.p,     c->ham.diag.p,    c->A.p,        c->X.p,
                         c->Y.p,          c->wf0.p,         c->partials.p, c->out.p,
@@ -1885,6 +2065,7 @@ void ham_upload(tbpm_ctx* c, const int32_t* indptr, const int32_t* indices, cons
   h.n = n;
   h.nnz = n_off;
   h.rescale = rescale;
+  ++h.gen;
 }
 
 }  // namespace

@@ -6,6 +6,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -63,6 +64,7 @@ struct Ham {
   bool has_dxy = false;
   bool has_diag = false;
   double rescale = 1.0;
+  uint64_t gen = 0;  // advanced by every upload or device build of a Hamiltonian
 };
 
 // Chebyshev-type expansion  out = sum_k w_k p_k,
@@ -97,6 +99,28 @@ struct GraphCache {
   ~GraphCache() { reset(); }
 };
 
+// Work plan of the paired-term kernel (tbpm_pair_kernels.cuh) for one tile
+// height: each tile's dependency list, the item sequence and the flags.
+// Built on the device for the current Hamiltonian (gen), rebuilt after the
+// next upload.
+struct PairPlan {
+  int rows = 0;          // rows per tile
+  int grid = 0;          // launch grid the sequence margin was set for
+  uint64_t ham_gen = 0;  // Hamiltonian it was built for
+  bool forced = false;   // built ignoring the L2 window test
+  bool usable = false;   // every list fits kPairDeps (and the window test passed)
+  int n_tiles = 0;
+  DevMem seq, deps, flags, sync;
+};
+
+// A plan asked for while a graph was being captured (it cannot be built
+// then: the build synchronises); ensure_graph builds it and captures again.
+struct PairRequest {
+  int rows, grid, stages;
+  size_t tile_bytes;
+  bool force;
+};
+
 struct Session {
   bool active = false;
   int kind = 0;  // 1 = DOS
@@ -119,6 +143,9 @@ struct tbpm_ctx {
   tbpm::DevMem raw;  // device copy of an uploaded host CSR, kept for the next upload
   tbpm::DevMem status;  // bit 0: a bounded device-side wait ran out (cleared when read)
   tbpm::DevMem anl;     // inputs and outputs of the Analyzer's trigonometric sums
+  std::vector<std::unique_ptr<tbpm::PairPlan>> pairs;  // paired-term plans, by tile height
+  std::vector<tbpm::PairRequest> pair_requests;
+  tbpm::DevMem pair_tmp;  // scratch of the plan build
   int64_t launches = 0;
   double model_bytes = 0;
   tbpm::Session sess;

@@ -747,6 +747,7 @@ void drv_supercell_ham(tbpm_ctx* c, const tbpm_supercell* sc, int layout, double
   h.n = n;
   h.nnz = n_off;
   h.rescale = P.rescale;
+  ++h.gen;
   if (n_rows) *n_rows = n;
   if (nnz) *nnz = n_off + (int64_t)n_diag;
   if (rescale) *rescale = P.rescale;

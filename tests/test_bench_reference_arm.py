@@ -59,3 +59,35 @@ def test_algorithmic_bytes_follow_the_flush_schedule(n_bes):
             b += vec
         want += b
     assert bench.algorithmic_bytes_per_step(n, nnz, ld, n_bes, rb) == want
+
+
+@pytest.mark.parametrize("n_bes", [4, 5, 7, 20, 21])
+@pytest.mark.parametrize("with_ref", [True, False])
+def test_paired_bytes_drop_the_second_terms_l2_reads(n_bes, with_ref):
+    """Paired terms (k, k+1) for k = 1, 3, ...: the second term of each pair
+    reads the CSR, p_k and its own p_{k-1} rows from L2, so each pair saves
+    the CSR and two vector passes; a last term with the correlation and two
+    flush terms in a row stay single."""
+    n, nnz, ld, rb = 1000, 3000, 16, 8
+    sv = 2 * rb
+    vec = n * ld * sv
+    mat = (n + 1) * 4 + nnz * (4 + sv)
+    flush, last = set(), -1
+    for k in range(2, n_bes):
+        if k == 2 or k - last == 3 or k == n_bes - 1:
+            flush.add(k)
+            last = k
+    pairs, k = 0, 1
+    while k < n_bes:
+        if k + 1 < n_bes and not (with_ref and k + 1 == n_bes - 1) and \
+                not (k in flush and k + 1 in flush):
+            pairs += 1
+            k += 2
+        else:
+            k += 1
+    single = bench.algorithmic_bytes_per_step(n, nnz, ld, n_bes, rb, with_ref=with_ref)
+    paired = bench.algorithmic_bytes_per_step(n, nnz, ld, n_bes, rb, paired=True,
+                                              with_ref=with_ref)
+    assert paired == pytest.approx(single - pairs * (mat + 2 * vec), rel=1e-15)
+    if n_bes == 20 and with_ref:
+        assert pairs == 9

@@ -251,3 +251,92 @@ def test_tiny_and_degenerate_hamiltonians(prec, tol, case):
     got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 20, 8, 1e-9)
     ref = oracle.tbpm_dos(bes, ip, ix, hv, 20, wf0=wf0)
     assert rel_err(got, ref) < tol
+
+
+def _launches():
+    return f2py._ctx().last_stats()[0]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_paired_terms_match_single_terms_bit_for_bit(g256, prec):
+    """Two Chebyshev terms per launch (cheb_pair_kernel: the second term of a
+    tile waits for the first term of every tile it couples to, and reads p_k
+    from L2) give the states of one term per launch (the ring kernel) bit for
+    bit, in fewer launches; automatic selection (0) picks the pairs here."""
+    h = g256.build_ham_csr()
+    n = h.shape[0]
+    wf0 = unit_states(16, n, seed=23)
+    bes = bessel_series(math.pi)
+    out, launches = {}, {}
+    for kernel in (2, 0, 3):
+        f2py.set_backend(precision=prec, term_kernel=kernel)
+        dos = f2py.tbpm_dos_states(bes, h.indptr, h.indices, h.data, wf0, 8, 4, 1e-9)
+        launches[kernel] = _launches()
+        psi = f2py.tbpm_psi_t(bes, h.indptr, h.indices, h.data, wf0[3], np.array([0, 5]), 5, 4,
+                              1e-9)
+        out[kernel] = (dos, psi)
+    f2py.set_backend(term_kernel=0)
+    for kernel in (0, 3):
+        assert np.array_equal(out[kernel][0], out[2][0])
+        assert np.array_equal(out[kernel][1], out[2][1])
+        assert launches[kernel] < 0.65 * launches[2]
+
+
+def test_paired_terms_ac_and_dc_bit_for_bit(g128):
+    """The AC block (48 columns, Fermi and time expansions) and the DC +/-
+    block (32 columns) through paired terms equal the single-term ring."""
+    ip, ix, hv, dx, dy = g128.build_ham_dxy()
+    n = ip.size - 1
+    wf0 = unit_states(16, n, seed=29)
+    bes = bessel_series(math.pi / 2)
+    beta = g128.rescale / (tb.KB * 3000.0)
+    tnr = 12
+    en_range = g128.energy_range
+    energies = np.array([0.5 * i * en_range / tnr - en_range / 2. for i in range(2 * tnr)])
+    sel = np.where((energies >= -8.0) & (energies <= 8.0))[0]
+    t_step = 2 * math.pi / en_range
+    out = {}
+    for kernel in (2, 0):
+        f2py.set_backend(term_kernel=kernel)
+        ac = f2py.tbpm_accond_states(bes, beta, 0.0, ip, ix, hv, g128.rescale, dx, dy, wf0, tnr,
+                                     2**15, 1e-12, 128, 1e-9)
+        dos, dc = f2py.tbpm_dccond_states(bes, ip, ix, hv, g128.rescale, dx, dy, wf0[:8], tnr,
+                                          t_step, energies, sel, 128, 1e-9)
+        out[kernel] = (ac, dos, dc)
+    f2py.set_backend(term_kernel=0)
+    for a, b in zip(out[0], out[2]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_paired_terms_with_far_couplings(prec, tol):
+    """A ring of 6,000 sites whose every site also couples to the site half
+    the ring away: each row tile depends on a tile far down the sequence, so
+    most second terms are placed after all first terms and wait on their
+    flags (term_kernel 3 pairs them regardless of the L2 window)."""
+    n = 6000
+    rows = {}
+    rng = np.random.default_rng(5)
+    for r in range(n):
+        ent = {(r + 1) % n: -1.0, (r - 1) % n: -1.0}
+        ent[(r + n // 2) % n] = 0.3 + 0.1j if r < n // 2 else 0.3 - 0.1j
+        ent[r] = rng.uniform(-0.5, 0.5)
+        rows[r] = sorted(ent.items())
+    ip = np.zeros(n + 1, dtype=np.int32)
+    for r in range(n):
+        ip[r + 1] = ip[r] + len(rows[r])
+    ix = np.array([c for r in range(n) for c, _ in rows[r]], dtype=np.int32)
+    hv = np.array([v for r in range(n) for _, v in rows[r]], dtype=np.complex128) / 3.0
+    wf0 = unit_states(16, n, seed=7)
+    bes = bessel_series(math.pi)
+    f2py.set_backend(precision=prec, term_kernel=3)
+    got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 16, 8, 1e-9)
+    launches = _launches()
+    f2py.set_backend(term_kernel=2)
+    single = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 16, 8, 1e-9)
+    launches_single = _launches()
+    f2py.set_backend(term_kernel=0)
+    ref = oracle.tbpm_dos(bes, ip, ix, hv, 16, wf0=wf0)
+    assert rel_err(got, ref) < tol
+    assert np.array_equal(got, single)
+    assert launches < 0.65 * launches_single
