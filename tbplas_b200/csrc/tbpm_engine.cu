@@ -452,7 +452,9 @@ void build_pair_plan(tbpm_ctx* c, PairPlan& p, const PairRequest& q) {
   TBPM_CK(cudaMemsetAsync(flags2, 0, 8, st));
   TBPM_CK(cudaMemsetAsync(p.flags.p, 0, (size_t)nt * 4, st));
   TBPM_CK(cudaMemsetAsync(p.sync.p, 0, sizeof(PairSync), st));
-  const int margin = q.grid * (q.stages + kPairBatch) / 2;
+  // a second term goes about two items per block (plus the stages in
+  // flight) after its last dependency, counted in first terms
+  const int margin = q.grid * (q.stages + 2) / 2;
   const long long window = (long long)(kPairL2Window / std::max<size_t>(3 * q.tile_bytes, 1));
   const int near = (int)std::max<long long>(0, std::min<long long>(window - margin, nt));
   const int gw = (int)std::min<int64_t>((nt + 7) / 8, (int64_t)kSMs * 16);
@@ -510,9 +512,19 @@ void launch_pair(tbpm_ctx* c, const PairPlan& pp, const RingShape& rs, const Ter
   pa.flags = pp.flags.as<unsigned>();
   pa.sync = pp.sync.as<PairSync>();
   pa.status = c->status.as<unsigned int>();
-  cheb_pair_kernel<R, V><<<pp.grid, kRingThreads, (size_t)rs.smem_bytes + kPairExtraSmem,
-                           c->stream>>>(pa);
-  TBPM_CK(cudaGetLastError());
+  // cooperative: every block of the grid is resident at once (the items of a
+  // block wait on items of other blocks)
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)pp.grid);
+  cfg.blockDim = dim3(kRingThreads);
+  cfg.dynamicSmemBytes = (size_t)rs.smem_bytes + kPairExtraSmem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  TBPM_CK(cudaLaunchKernelEx(&cfg, cheb_pair_kernel<R, V>, pa));
   c->launches++;
 }
 

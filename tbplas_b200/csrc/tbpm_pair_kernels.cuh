@@ -19,13 +19,13 @@
 // tiles whose rows read it (the transposed pattern): its second term runs
 // only after the first term of every tile on the list, which covers both.
 //
-// Items are handed out in the order of a precomputed sequence (pair_seq_kernel):
-// all first terms in tile order, each second term placed after the first
-// terms of its whole list plus a margin of about the work in flight.  Every
-// dependency of an item lies earlier in the sequence, and a block takes items
-// in sequence order (kPairBatch at a time from an atomic counter), so the
-// earliest unfinished item can always proceed: no deadlock, whatever the
-// number of resident blocks.
+// Items follow a precomputed sequence (pair_seq_kernel): all first terms in
+// tile order, each second term placed after the first terms of its whole list
+// plus a margin of about the work in flight.  Block b takes positions b, b+G,
+// b+2G, ... in order (G blocks, launched cooperatively, so all are resident).
+// Every dependency of an item lies earlier in the sequence and a producer
+// stores the flags of its finished items before it waits on anything, so the
+// earliest unfinished item can always proceed: the waits cannot deadlock.
 //
 // A block is one producer warp and kRingConsumerWarps consumer warps around a
 // ring of shared-memory stages, as in cheb_ring_kernel.  The producer stages
@@ -34,8 +34,10 @@
 // during the launch, is read by the consumers with L2-only loads (ld.global.cg)
 // after the producer has seen the flags of the item's dependencies; the flags
 // are set by the producer (release, GPU scope) once all consumer warps have
-// arrived on the stage's "empty" mbarrier for a first-term item.  Flags hold
-// the launch number + 1 (PairSync::epoch), so they never need resetting.
+// arrived on the stage's "empty" mbarrier for a first-term item, up to
+// kPairPend of them after one fence, which a second term's acquire fence also
+// serves.  Flags hold the launch number + 1 (PairSync::epoch), so they never
+// need resetting.
 //
 // Every wait is bounded in time (kRingWaitNs) and also ends when another block
 // has reported a failure; a wait that runs out sets bit 0 of *status.
@@ -46,15 +48,14 @@
 namespace tbpm {
 
 constexpr int kPairDeps = 16;   // dependency tiles per tile (padded with -1)
-constexpr int kPairBatch = 4;   // items a producer takes per atomic
+constexpr int kPairPend = 8;    // first-term flags a producer stores after one fence
 constexpr int kPairEnd = -1;    // stage marker: no more items
-constexpr int kPairExtraSmem = 64;  // item codes of the stages, after the mbarriers
+constexpr int kPairExtraSmem = 128;  // stage item codes, flag value, pending flags
 
 struct PairSync {
-  unsigned epoch;    // launches completed with this plan
-  unsigned counter;  // next item to hand out
-  unsigned done;     // blocks finished in the current launch
-  unsigned pad;
+  unsigned epoch;  // launches completed with this plan
+  unsigned done;   // blocks finished in the current launch
+  unsigned pad[2];
 };
 
 template <typename R, int V>
@@ -86,8 +87,8 @@ __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   return v;
 }
 
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // Producer: stage the operands of one item (lane 0 only).  Own rows of
@@ -273,10 +274,12 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
   const unsigned FULL = 0xffffffffu;
   const uint32_t full0 = ring_smem(rsm + sh.bar_off);
   const uint32_t empty0 = full0 + 8u * (uint32_t)S;
-  // after the mbarriers: the item code of each stage, then this launch's flag value
+  // after the mbarriers: the item code of each stage (8 at most), this
+  // launch's flag value, the producer's pending flags
   volatile int* item_of = reinterpret_cast<volatile int*>(rsm + sh.bar_off + 16 * S);
   volatile unsigned* want_p =
       reinterpret_cast<volatile unsigned*>(rsm + sh.bar_off + 16 * S + 32);
+  volatile int* pend = reinterpret_cast<volatile int*>(rsm + sh.bar_off + 16 * S + 64);
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -292,88 +295,97 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
   if (tid >= kRingConsumers) {
     // ---------------- producer warp ----------------
     const int wl = tid & 31;
+    const int64_t G = gridDim.x;
+    const int64_t n_items = pa.n_items;
     bool ok = true;
-    int64_t issued = 0, pub = 0;
+    int64_t issued = 0, pub = 0;  // items issued; items seen done (all of [0, pub))
+    int n_pend = 0;               // first-term items seen done whose flags are not stored yet
     auto failed_elsewhere = [&]() {
       return *reinterpret_cast<volatile unsigned*>(pa.status) != 0u;
     };
-    // Publish items [pub, upto) whose consumers are done: the flag of a
-    // first-term item is set once all consumer warps have stored its rows.
-    // block = false stops at the first item still in progress.
-    auto publish = [&](int64_t upto, bool block) -> bool {
+    // Store the pending flags after one fence (the release pattern: the
+    // consumers' rows, seen through the empty mbarriers, before the flags).
+    auto flush = [&]() {
+      if (n_pend > 0) {
+        if (wl == 0) {
+          asm volatile("fence.acq_rel.gpu;" ::: "memory");
+          for (int i = 0; i < n_pend; ++i) st_relaxed_u32(pa.flags + pend[i], want);
+        }
+        __syncwarp();
+        n_pend = 0;
+      }
+    };
+    // Observe items [pub, upto) done; block = false stops at the first item
+    // still in progress.  Returns whether all of them are done (blocking: false
+    // when a wait ran out).
+    auto observe = [&](int64_t upto, bool block) -> bool {
       while (pub < upto) {
         const int s = (int)(pub % S);
         const uint32_t par = (uint32_t)((pub / S) & 1);
         const bool done = block ? __all_sync(FULL, ring_wait(empty0 + 8u * s, par))
                                 : __all_sync(FULL, ring_test(empty0 + 8u * s, par));
-        if (!done) return !block;
-        if (wl == 0) {
-          const int code = item_of[s];
-          if ((code & 1) == 0) {
-            asm volatile("fence.acq_rel.gpu;" ::: "memory");
-            st_release_u32(pa.flags + (code >> 1), want);
-          }
+        if (!done) return false;
+        const int code = item_of[s];
+        if ((code & 1) == 0) {
+          if (wl == 0) pend[n_pend] = code >> 1;
+          __syncwarp();
+          if (++n_pend == kPairPend) flush();
         }
-        __syncwarp();
         ++pub;
       }
       return true;
     };
-    auto grab = [&]() -> unsigned {  // valid in lane 0
-      unsigned b = 0;
-      if (wl == 0) b = atomicAdd(&pa.sync->counter, (unsigned)kPairBatch);
-      return b;
+    // Item q of this block is sequence position blockIdx.x + q * G; lane l
+    // holds the entry of item wbase + l, and of wbase + 32 + l (next window).
+    auto entry = [&](int64_t q) -> int4 {
+      const int64_t p = (int64_t)blockIdx.x + q * G;
+      return p < n_items ? pa.seq[p] : make_int4(kPairEnd, 0, 0, 0);
     };
-    const unsigned n_items = (unsigned)pa.n_items;
-    auto entry = [&](unsigned base) -> int4 {  // lane j < kPairBatch: item base + j
-      int4 e = make_int4(kPairEnd, 0, 0, 0);
-      if (wl < kPairBatch && base < n_items && base + (unsigned)wl < n_items)
-        e = pa.seq[base + (unsigned)wl];
-      return e;
+    int64_t wbase = 0;
+    int4 e_cur = entry(wl), e_nxt = entry(32 + wl);
+    auto code_at = [&](int64_t q) -> int {  // q in [wbase, wbase + 64)
+      const int d = (int)(q - wbase);
+      const int c0 = __shfl_sync(FULL, e_cur.x, d & 31);
+      const int c1 = __shfl_sync(FULL, e_nxt.x, d & 31);
+      return d < 32 ? c0 : c1;
     };
     auto dep_row = [&](int code) -> int {  // lane's dependency of a second-term item
       return (code >= 0 && (code & 1) && wl < kPairDeps) ? pa.deps[(code >> 1) * kPairDeps + wl]
                                                           : -1;
     };
-    // item q + d's entry from the current (j + d < kPairBatch) or the next batch
-    auto look = [&](const int4& cur, const int4& nxt, int j, int d) -> int {
-      const int jj = j + d;
-      const int from_cur = __shfl_sync(FULL, cur.x, jj < kPairBatch ? jj : 0);
-      const int from_nxt = __shfl_sync(FULL, nxt.x, jj < kPairBatch ? 0 : jj - kPairBatch);
-      return jj < kPairBatch ? from_cur : from_nxt;
-    };
-    unsigned b_nxt;
-    int4 e_cur, e_nxt;
-    {
-      const unsigned b_cur = __shfl_sync(FULL, grab(), 0);
-      b_nxt = __shfl_sync(FULL, grab(), 0);
-      e_cur = entry(b_cur);
-      e_nxt = entry(b_nxt);
-    }
-    unsigned g_after = grab();
     // dependency rows and flag values, loaded one and two items ahead
-    int dep0 = dep_row(look(e_cur, e_nxt, 0, 0));
+    int dep0 = dep_row(code_at(0));
     unsigned fl0 = dep0 >= 0 ? ld_relaxed_u32(pa.flags + dep0) : want;
-    int dep1 = dep_row(look(e_cur, e_nxt, 0, 1));
+    int dep1 = dep_row(code_at(1));
     for (int64_t q = 0;; ++q) {
-      const int j = (int)(q % kPairBatch);
-      const int code = __shfl_sync(FULL, e_cur.x, j);
-      const int j0 = __shfl_sync(FULL, e_cur.y, j);
-      const int j1 = __shfl_sync(FULL, e_cur.z, j);
+      if (q == wbase + 32) {
+        e_cur = e_nxt;
+        wbase += 32;
+        e_nxt = entry(wbase + 32 + wl);
+      }
+      const int d = (int)(q - wbase);
+      const int code = __shfl_sync(FULL, e_cur.x, d);
+      const int j0 = __shfl_sync(FULL, e_cur.y, d);
+      const int j1 = __shfl_sync(FULL, e_cur.z, d);
       if (code < 0) break;
       const int s = (int)(q % S);
-      // the stage is free once the item S back is done (and published)
-      if (q >= S && !publish(q - S + 1, true)) {
-        ok = false;
-        break;
+      // the stage is free once the item S back is done; flags go out before
+      // any wait, so no other block waits on this one while it waits
+      if (q >= S && !observe(q - S + 1, false)) {
+        flush();
+        if (!observe(q - S + 1, true)) {
+          ok = false;
+          break;
+        }
       }
-      publish(issued, false);
+      observe(issued, false);
       if (code & 1) {
         // second term: the first term of every dependency must be stored
         if (!__all_sync(FULL, fl0 == want)) {
           const unsigned long long t0 = ring_clock_ns();
           for (;;) {
-            publish(issued, false);
+            observe(issued, false);
+            flush();
             fl0 = dep0 >= 0 ? ld_relaxed_u32(pa.flags + dep0) : want;
             if (__all_sync(FULL, fl0 == want)) break;
             bool out = ring_clock_ns() - t0 > kRingWaitNs || failed_elsewhere();
@@ -385,7 +397,13 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           }
           if (!ok) break;
         }
+        // one fence: acquire for the flags read above, release for the
+        // pending flags stored below
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        if (wl == 0)
+          for (int i = 0; i < n_pend; ++i) st_relaxed_u32(pa.flags + pend[i], want);
+        __syncwarp();
+        n_pend = 0;
       }
       if (wl == 0) {
         char* st = rsm + (size_t)s * sh.stage_bytes;
@@ -401,23 +419,20 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
       ++issued;
       // look-ahead: flags of item q+1, dependency row of item q+2
       const unsigned fl1 = dep1 >= 0 ? ld_relaxed_u32(pa.flags + dep1) : want;
-      const int dep2 = dep_row(look(e_cur, e_nxt, j, 2));
+      const int dep2 = dep_row(code_at(q + 2));
       dep0 = dep1;
       fl0 = fl1;
       dep1 = dep2;
-      if (j == kPairBatch - 1) {
-        e_cur = e_nxt;
-        b_nxt = __shfl_sync(FULL, g_after, 0);
-        e_nxt = entry(b_nxt);
-        g_after = grab();
-      }
     }
     // no more items: mark the next stage as the end for the consumers, then
     // publish everything still pending
     bool end_sent = false;
     if (ok) {
       const int64_t q = issued;
-      if (q >= S && !publish(q - S + 1, true)) ok = false;
+      if (q >= S && !observe(q - S + 1, false)) {
+        flush();
+        if (!observe(q - S + 1, true)) ok = false;
+      }
       if (ok) {
         if (wl == 0) {
           item_of[(int)(q % S)] = kPairEnd;
@@ -425,9 +440,15 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
         }
         __syncwarp();
         end_sent = true;
-        if (!publish(issued, true)) ok = false;
+        while (ok && pub < issued) {
+          if (!observe(issued, false)) {
+            flush();
+            if (!observe(issued, true)) ok = false;
+          }
+        }
       }
     }
+    flush();
     if (!ok) {
       if (wl == 0) atomicOr(pa.status, 1u);
       // let the consumers stop at the next stage when it is free
@@ -462,14 +483,13 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     }
   }
 
-  // the last block to finish resets the hand-out counter and advances the epoch
+  // the last block to finish advances the epoch
   __syncthreads();
   if (tid == 0) {
     __threadfence();
     const unsigned prev = atomicAdd(&pa.sync->done, 1u);
     if (prev == gridDim.x - 1) {
       pa.sync->done = 0u;
-      pa.sync->counter = 0u;
       __threadfence();
       pa.sync->epoch = want;
     }
