@@ -21,8 +21,9 @@
 //
 // Items follow a precomputed sequence (pair_seq_kernel): all first terms in
 // tile order, each second term placed after the first terms of its whole list
-// plus a margin of about the work in flight.  Block b takes positions b, b+G,
-// b+2G, ... in order (G blocks, launched cooperatively, so all are resident).
+// plus a margin of about the work in flight.  Block b takes one position of
+// each round of G positions, in order (G blocks, launched cooperatively, so
+// all are resident).
 // Every dependency of an item lies earlier in the sequence and a producer
 // stores the flags of its finished items before it waits on anything, so the
 // earliest unfinished item can always proceed: the waits cannot deadlock.
@@ -335,10 +336,13 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
       }
       return true;
     };
-    // Item q of this block is sequence position blockIdx.x + q * G; lane l
-    // holds the entry of item wbase + l, and of wbase + 32 + l (next window).
+    // Item q of this block is sequence position q * G + (blockIdx.x + q) % G:
+    // round q of the sequence, at an offset that turns with the round, so a
+    // block alternates between first and second terms where they alternate in
+    // the sequence (a plain stride of an even G would give a block only one
+    // kind).  Lane l holds the entry of item wbase + l, and of wbase + 32 + l.
     auto entry = [&](int64_t q) -> int4 {
-      const int64_t p = (int64_t)blockIdx.x + q * G;
+      const int64_t p = q * G + ((int64_t)blockIdx.x + q) % G;
       return p < n_items ? pa.seq[p] : make_int4(kPairEnd, 0, 0, 0);
     };
     int64_t wbase = 0;
