@@ -636,10 +636,9 @@ def main():
                     help="FP64 complex values per thread: 0 library default (two, 256-bit "
                          "accesses), 1 one (128-bit accesses), 2 two")
     ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="Chebyshev-term kernel: 0 library default (two terms per launch "
-                         "where the dependency lists allow, else the shared-memory ring), "
-                         "1 grid-stride kernel with plain loads, 2 ring (one term per "
-                         "launch), 3 two terms per launch wherever the lists fit")
+                    help="Chebyshev-term kernel: 0 library default (shared-memory ring fed by "
+                         "bulk copies), 1 grid-stride kernel with plain loads, 2 ring, 3 two "
+                         "terms per launch")
     ap.add_argument("--threads", type=int, default=0,
                     help="FP64 threads per block of the term kernel (0: library default)")
     ap.add_argument("--nx", type=int, default=2048,

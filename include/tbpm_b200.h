@@ -68,15 +68,15 @@ typedef struct tbpm_options {
                             multiple of 4, else 2 when even), 1, 2.  FP64: 0 = automatic
                             (two complex128 per thread with 256-bit accesses when the
                             block width allows), 1 = one (128-bit accesses), 2 */
-  int term_kernel;       /* Chebyshev-term kernel: 0 = automatic (two terms per
-                            launch where every row tile couples to at most 16
-                            tiles and the rows between a tile's two terms fit the
-                            L2 window, else the shared-memory ring fed by bulk
-                            copies wherever a row of the state block is a
-                            multiple of 16 bytes, else the grid-stride kernel),
-                            1 = the grid-stride kernel with plain loads, 2 = the
-                            ring, one term per launch, 3 = two terms per launch
-                            wherever the dependency lists fit */
+  int term_kernel;       /* Chebyshev-term kernel: 0 = automatic (the shared-memory
+                            ring fed by bulk copies wherever a row of the state
+                            block is a multiple of 16 bytes, else the grid-stride
+                            kernel), 1 = the grid-stride kernel with plain loads,
+                            2 = the ring where it applies, 3 = two terms per
+                            launch (the second term of a tile after the first
+                            term of every tile it couples to, p_k read back from
+                            L2) where every tile couples to at most 16 tiles;
+                            slower than the ring on the measured workloads */
   double dc_budget_gb;   /* device memory (GiB) the DC driver may give its quasi-
                             eigenstate block and state ring; 0 = the free memory.
                             Fewer states per batch, then energy chunks (each

@@ -406,6 +406,9 @@ int pair_blocks_per_sm(const tbpm_ctx* c, size_t smem) {
   return resident_per_sm(cheb_pair_kernel<R, V>, kRingThreads, smem);
 }
 
+#ifndef TBPM_PAIR_LAG
+#define TBPM_PAIR_LAG 2
+#endif
 // L2 the rows between a tile's two terms may occupy: the second term finds
 // p_k, p_{k-1} and the CSR slice of its tile in L2 while the tiles started
 // in between (the margin plus the dependency lag) fit in this budget.
@@ -452,9 +455,9 @@ void build_pair_plan(tbpm_ctx* c, PairPlan& p, const PairRequest& q) {
   TBPM_CK(cudaMemsetAsync(flags2, 0, 8, st));
   TBPM_CK(cudaMemsetAsync(p.flags.p, 0, (size_t)nt * 4, st));
   TBPM_CK(cudaMemsetAsync(p.sync.p, 0, sizeof(PairSync), st));
-  // a second term goes about two items per block (plus the stages in
+  // a second term goes TBPM_PAIR_LAG items per block (plus the stages in
   // flight) after its last dependency, counted in first terms
-  const int margin = q.grid * (q.stages + 2) / 2;
+  const int margin = q.grid * (q.stages + TBPM_PAIR_LAG) / 2;
   const long long window = (long long)(kPairL2Window / std::max<size_t>(3 * q.tile_bytes, 1));
   const int near = (int)std::max<long long>(0, std::min<long long>(window - margin, nt));
   const int gw = (int)std::min<int64_t>((nt + 7) / 8, (int64_t)kSMs * 16);
@@ -517,7 +520,7 @@ void launch_pair(tbpm_ctx* c, const PairPlan& pp, const RingShape& rs, const Ter
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)pp.grid);
   cfg.blockDim = dim3(kRingThreads);
-  cfg.dynamicSmemBytes = (size_t)rs.smem_bytes + kPairExtraSmem;
+  cfg.dynamicSmemBytes = (size_t)rs.smem_bytes + pair_extra_smem<R, V>();
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -605,15 +608,18 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
     }
     term_bytes[k] = bytes;
   }
-  // Terms k, k+1 run as one paired launch where the plan applies, except a
-  // last term with correlation partials and two flush terms in a row (the
-  // second would stage accumulator rows the first wrote in the same launch).
+  // With term_kernel 3, terms k, k+1 run as one paired launch where the plan
+  // applies, except a last term with correlation partials and two flush terms
+  // in a row (the second would stage accumulator rows the first wrote in the
+  // same launch).  (Measured on B200, 2048^2 graphene: the paired launches
+  // move the bytes of the model but take longer than two ring launches; the
+  // automatic choice is the ring.)
   PairPlan* pp = nullptr;
   RingShape prs{};
   const int tk = c->opts.term_kernel;
-  if (n >= 3 && (tk == 0 || tk == 3) && tt.ring[1]) {
+  if (n >= 3 && tk == 3 && tt.ring[1]) {
     prs = tt.rs[1];
-    const size_t smem = (size_t)prs.smem_bytes + kPairExtraSmem;
+    const size_t smem = (size_t)prs.smem_bytes + pair_extra_smem<R, V>();
     if (smem <= 227 * 1024) {
       const int per_sm = pair_blocks_per_sm<R, V>(c, smem);
       const int64_t tiles = (h.n + prs.rows - 1) / prs.rows;
@@ -623,7 +629,7 @@ void enqueue_expansion(tbpm_ctx* c, const Expansion& ex, int ld, Pack<R, V>* A, 
           1, std::min<int64_t>((int64_t)per_sm * num_sms(c->device), tiles));
       q.stages = prs.stages;
       q.tile_bytes = (size_t)prs.rows * tpr * sizeof(Pack<R, V>);
-      q.force = tk == 3;
+      q.force = true;
       pp = pair_plan(c, q);
     }
   }

@@ -24,21 +24,20 @@
 // plus a margin of about the work in flight.  Block b takes one position of
 // each round of G positions, in order (G blocks, launched cooperatively, so
 // all are resident).
-// Every dependency of an item lies earlier in the sequence and a producer
-// stores the flags of its finished items before it waits on anything, so the
-// earliest unfinished item can always proceed: the waits cannot deadlock.
+// Every dependency of an item lies earlier in the sequence and the flag of a
+// finished item is stored by its consumers, whatever its producer waits on,
+// so the earliest unfinished item can always proceed: no deadlock.
 //
 // A block is one producer warp and kRingConsumerWarps consumer warps around a
 // ring of shared-memory stages, as in cheb_ring_kernel.  The producer stages
 // each item's CSR slice, diagonal, p_{k-2} / p_{k-1} rows and accumulator by
 // bulk copies (data that no block writes during the launch).  p_k, written
 // during the launch, is read by the consumers with L2-only loads (ld.global.cg)
-// after the producer has seen the flags of the item's dependencies; the flags
-// are set by the producer (release, GPU scope) once all consumer warps have
-// arrived on the stage's "empty" mbarrier for a first-term item, up to
-// kPairPend of them after one fence, which a second term's acquire fence also
-// serves.  Flags hold the launch number + 1 (PairSync::epoch), so they never
-// need resetting.
+// after the producer has seen the flags of the item's dependencies (relaxed
+// loads, then one acquire fence per second-term item).  The last consumer
+// warp done with a first-term item (an acq_rel counter in shared memory)
+// stores the tile's flag after a GPU-scope fence.  Flags hold the launch
+// number + 1 (PairSync::epoch), so they never need resetting.
 //
 // Every wait is bounded in time (kRingWaitNs) and also ends when another block
 // has reported a failure; a wait that runs out sets bit 0 of *status.
@@ -49,9 +48,13 @@
 namespace tbpm {
 
 constexpr int kPairDeps = 16;   // dependency tiles per tile (padded with -1)
-constexpr int kPairPend = 8;    // first-term flags a producer stores after one fence
 constexpr int kPairEnd = -1;    // stage marker: no more items
-constexpr int kPairExtraSmem = 128;  // stage item codes, flag value, pending flags
+// after the mbarriers: stage item codes, flag value, per-stage counts of
+// consumer warps done (128 bytes), then the two terms' arguments
+template <typename R, int V>
+constexpr int pair_extra_smem() {
+  return 128 + 2 * (int)((sizeof(TermArgs<R, V>) + 15) / 16 * 16);
+}
 
 struct PairSync {
   unsigned epoch;  // launches completed with this plan
@@ -276,11 +279,17 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
   const uint32_t full0 = ring_smem(rsm + sh.bar_off);
   const uint32_t empty0 = full0 + 8u * (uint32_t)S;
   // after the mbarriers: the item code of each stage (8 at most), this
-  // launch's flag value, the producer's pending flags
+  // launch's flag value, the consumer warps done with each stage's item
   volatile int* item_of = reinterpret_cast<volatile int*>(rsm + sh.bar_off + 16 * S);
   volatile unsigned* want_p =
       reinterpret_cast<volatile unsigned*>(rsm + sh.bar_off + 16 * S + 32);
-  volatile int* pend = reinterpret_cast<volatile int*>(rsm + sh.bar_off + 16 * S + 64);
+  unsigned* done_cnt = reinterpret_cast<unsigned*>(rsm + sh.bar_off + 16 * S + 64);
+  // the consumers read the arguments of an item's term from shared memory (a
+  // runtime index into the kernel parameters costs a dependent load per field)
+  constexpr int kArgBytes = (int)((sizeof(TermArgs<R, V>) + 15) / 16 * 16);
+  TermArgs<R, V>* args = reinterpret_cast<TermArgs<R, V>*>(rsm + sh.bar_off + 16 * S + 128);
+  TermArgs<R, V>* args1 =
+      reinterpret_cast<TermArgs<R, V>*>(rsm + sh.bar_off + 16 * S + 128 + kArgBytes);
 
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
@@ -289,7 +298,10 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     *want_p = ld_relaxed_u32(&pa.sync->epoch) + 1u;
+    *args = pa.t[0];
+    for (int s = 0; s < S; ++s) done_cnt[s] = 0u;
   }
+  if (tid == 32) *args1 = pa.t[1];
   __syncthreads();
   const unsigned want = *want_p;
 
@@ -299,42 +311,9 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     const int64_t G = gridDim.x;
     const int64_t n_items = pa.n_items;
     bool ok = true;
-    int64_t issued = 0, pub = 0;  // items issued; items seen done (all of [0, pub))
-    int n_pend = 0;               // first-term items seen done whose flags are not stored yet
+    int64_t issued = 0;
     auto failed_elsewhere = [&]() {
       return *reinterpret_cast<volatile unsigned*>(pa.status) != 0u;
-    };
-    // Store the pending flags after one fence (the release pattern: the
-    // consumers' rows, seen through the empty mbarriers, before the flags).
-    auto flush = [&]() {
-      if (n_pend > 0) {
-        if (wl == 0) {
-          asm volatile("fence.acq_rel.gpu;" ::: "memory");
-          for (int i = 0; i < n_pend; ++i) st_relaxed_u32(pa.flags + pend[i], want);
-        }
-        __syncwarp();
-        n_pend = 0;
-      }
-    };
-    // Observe items [pub, upto) done; block = false stops at the first item
-    // still in progress.  Returns whether all of them are done (blocking: false
-    // when a wait ran out).
-    auto observe = [&](int64_t upto, bool block) -> bool {
-      while (pub < upto) {
-        const int s = (int)(pub % S);
-        const uint32_t par = (uint32_t)((pub / S) & 1);
-        const bool done = block ? __all_sync(FULL, ring_wait(empty0 + 8u * s, par))
-                                : __all_sync(FULL, ring_test(empty0 + 8u * s, par));
-        if (!done) return false;
-        const int code = item_of[s];
-        if ((code & 1) == 0) {
-          if (wl == 0) pend[n_pend] = code >> 1;
-          __syncwarp();
-          if (++n_pend == kPairPend) flush();
-        }
-        ++pub;
-      }
-      return true;
     };
     // Item q of this block is sequence position q * G + (blockIdx.x + q) % G:
     // round q of the sequence, at an offset that turns with the round, so a
@@ -373,23 +352,17 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
       const int j1 = __shfl_sync(FULL, e_cur.z, d);
       if (code < 0) break;
       const int s = (int)(q % S);
-      // the stage is free once the item S back is done; flags go out before
-      // any wait, so no other block waits on this one while it waits
-      if (q >= S && !observe(q - S + 1, false)) {
-        flush();
-        if (!observe(q - S + 1, true)) {
-          ok = false;
-          break;
-        }
+      // the stage is free once the consumers are done with the item S back
+      if (q >= S &&
+          !__all_sync(FULL, ring_wait(empty0 + 8u * s, (uint32_t)(((q / S) + 1) & 1)))) {
+        ok = false;
+        break;
       }
-      observe(issued, false);
       if (code & 1) {
         // second term: the first term of every dependency must be stored
         if (!__all_sync(FULL, fl0 == want)) {
           const unsigned long long t0 = ring_clock_ns();
           for (;;) {
-            observe(issued, false);
-            flush();
             fl0 = dep0 >= 0 ? ld_relaxed_u32(pa.flags + dep0) : want;
             if (__all_sync(FULL, fl0 == want)) break;
             bool out = ring_clock_ns() - t0 > kRingWaitNs || failed_elsewhere();
@@ -401,13 +374,8 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           }
           if (!ok) break;
         }
-        // one fence: acquire for the flags read above, release for the
-        // pending flags stored below
+        // acquire: the dependencies' rows of p_k before the consumers' loads
         asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        if (wl == 0)
-          for (int i = 0; i < n_pend; ++i) st_relaxed_u32(pa.flags + pend[i], want);
-        __syncwarp();
-        n_pend = 0;
       }
       if (wl == 0) {
         char* st = rsm + (size_t)s * sh.stage_bytes;
@@ -428,42 +396,37 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
       fl0 = fl1;
       dep1 = dep2;
     }
-    // no more items: mark the next stage as the end for the consumers, then
-    // publish everything still pending
+    // no more items: mark the next stage as the end for the consumers
     bool end_sent = false;
     if (ok) {
       const int64_t q = issued;
-      if (q >= S && !observe(q - S + 1, false)) {
-        flush();
-        if (!observe(q - S + 1, true)) ok = false;
-      }
+      const int s = (int)(q % S);
+      if (q >= S &&
+          !__all_sync(FULL, ring_wait(empty0 + 8u * s, (uint32_t)(((q / S) + 1) & 1))))
+        ok = false;
       if (ok) {
         if (wl == 0) {
-          item_of[(int)(q % S)] = kPairEnd;
-          ring_arrive(full0 + 8u * (int)(q % S));
+          item_of[s] = kPairEnd;
+          ring_arrive(full0 + 8u * s);
         }
         __syncwarp();
         end_sent = true;
-        while (ok && pub < issued) {
-          if (!observe(issued, false)) {
-            flush();
-            if (!observe(issued, true)) ok = false;
-          }
-        }
       }
     }
-    flush();
+    // (after the end marker the consumers wait for every issued stage, so
+    // its copies land before the block ends)
     if (!ok) {
       if (wl == 0) atomicOr(pa.status, 1u);
-      // let the consumers stop at the next stage when it is free
-      if (!end_sent && (issued < S || pub > issued - S)) {
+      if (!end_sent && issued < S) {
         if (wl == 0) {
           item_of[(int)(issued % S)] = kPairEnd;
           ring_arrive(full0 + 8u * (int)(issued % S));
         }
       }
-      // the copies already issued must land before the block may end
-      for (int64_t i = pub; i < issued; ++i)
+      // consumers may have stopped: the copies already issued must land
+      // before the block may end
+      const int64_t first = issued > S ? issued - S : 0;
+      for (int64_t i = first; i < issued; ++i)
         if (!ring_wait(full0 + 8u * (int)(i % S), (uint32_t)((i / S) & 1))) break;
     }
   } else {
@@ -481,9 +444,26 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
       if (code < 0) break;
       const char* st = rsm + (size_t)s * sh.stage_bytes;
       const int64_t r0 = (int64_t)(code >> 1) * TR;
-      pair_rows<R, V>(pa.t[code & 1], sh, st, r0, slot, lane, (code & 1) != 0);
+      pair_rows<R, V>((code & 1) ? *args1 : *args, sh, st, r0, slot, lane, (code & 1) != 0);
       __syncwarp();
-      if ((tid & 31) == 0) ring_arrive(empty0 + 8u * s);
+      if ((tid & 31) == 0) {
+        if ((code & 1) == 0) {
+          // the last consumer warp done with a first-term item stores its flag:
+          // the warps' rows (acq_rel count in shared memory), then one fence
+          // and the flag (the release pattern at GPU scope)
+          unsigned prev;
+          asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;"
+                       : "=r"(prev)
+                       : "r"(ring_smem(done_cnt + s))
+                       : "memory");
+          if (prev == (unsigned)kRingConsumerWarps - 1u) {
+            done_cnt[s] = 0u;
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            st_relaxed_u32(pa.flags + (code >> 1), want);
+          }
+        }
+        ring_arrive(empty0 + 8u * s);
+      }
     }
   }
 
