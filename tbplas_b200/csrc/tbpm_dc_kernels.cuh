@@ -512,154 +512,6 @@ __global__ void __launch_bounds__(256, TBPM_QE_MINB_P) qe_project_kernel(
   }
 }
 
-// ---- quasi-eigenstate projections as FP64 matrix products (mma.sync) -------
-//
-// For a state b the projections of qe_project_kernel over the rows r of a
-// block's range are one real product  A (32 x 2R) . B (2R x energies):  row
-// mm = 2m + c of A (m = tau*K + k, c = re/im of the result) and column
-// (r, part) of B = Re / Im QE[r][i][b],
-//   A[2m][(r,0)] =  Re u,  A[2m][(r,1)] = Im u,
-//   A[2m+1][(r,0)] = -Im u, A[2m+1][(r,1)] = Re u,   u = u_tau[r][k*nb + b]
-// (wf0[r][b] in mode 1), which gives sum_r conj(u) QE.  A block covers the
-// rows of its range and the energies of kQePjNT tiles of 8 for every state; it
-// stages chunks of kQePjRows rows (the block's QE slice, contiguous per row,
-// and the rows' u values) into shared memory with cp.async, double-buffered,
-// and its warps build their mma.sync m8n8k4 f64 fragments from there: a warp
-// owns (state, energy tile) tasks and keeps their 4 x 8 accumulators in
-// registers over the whole range.  The block partials have the layout of
-// qe_project_kernel.
-constexpr int kQePjRows = 8;    // rows per staged chunk (4 k-steps)
-constexpr int kQePjTasks = 2;   // (state, energy tile) tasks per warp
-
-__host__ __device__ constexpr int qe_pj_tiles(int nb) {
-  // energy tiles per block: about kQeMmaWarps * kQePjTasks tasks for nb states
-  return nb >= kQeMmaWarps * kQePjTasks ? 1 : (kQeMmaWarps * kQePjTasks) / nb;
-}
-template <typename R>
-__host__ __device__ constexpr size_t qe_pj_smem(int nb) {
-  return 2 * (size_t)kQePjRows *
-         ((size_t)qe_pj_tiles(nb) * 8 * nb + (size_t)kMaxProject * 2 * nb) * 2 * sizeof(R);
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kQeMmaWarps * 32, 1) qe_project_mma_kernel(
-    const typename Cx<R>::t* qe, int64_t n_rows, int64_t rows_per_tile, int n_en, int nb,
-    const __grid_constant__ StatePtrs<R> u, int T, int mode, const typename Cx<R>::t* wf0,
-    double* partials) {
-  using C = typename Cx<R>::t;
-  extern __shared__ double2 qsm[];
-  const int64_t r0 = (int64_t)blockIdx.x * rows_per_tile;
-  const int64_t r1 = min(r0 + rows_per_tile, n_rows);
-  const int n_ib = n_en * nb;
-  const int K = mode == 0 ? 2 : 1;
-  const int M = mode == 0 ? T * K : 1;  // complex results per element
-  const int ld = 2 * nb;
-  const int UW = mode == 0 ? T * ld : nb;  // staged u values of a row
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int NTB = qe_pj_tiles(nb);
-  const int i0 = blockIdx.y * NTB * 8;             // first energy of the block
-  const int NE = min(NTB * 8, n_en - i0);          // energies of the block
-  const int QW = NE * nb;                          // staged QE values of a row
-  const int QWmax = NTB * 8 * nb;
-  C* sq = reinterpret_cast<C*>(qsm);               // [2][kQePjRows][QWmax]
-  C* su = sq + 2 * kQePjRows * QWmax;              // [2][kQePjRows][kMaxProject * ld]
-  const int UWmax = kMaxProject * ld;
-  auto issue = [&](int64_t rb, int buf) {
-    const int nr = (int)min((int64_t)kQePjRows, r1 - rb);
-    C* dq = sq + buf * kQePjRows * QWmax;
-    for (int q = threadIdx.x; q < nr * QW; q += blockDim.x) {
-      const int rr = q / QW, e = q - rr * QW;
-      qe_cp_async(dq + rr * QWmax + e, qe + ((rb + rr) * n_en + i0) * nb + e);
-    }
-    C* du = su + buf * kQePjRows * UWmax;
-    for (int q = threadIdx.x; q < nr * UW; q += blockDim.x) {
-      const int rr = q / UW, e = q - rr * UW;
-      const C* src = mode == 0 ? u.p[e / ld] + (rb + rr) * ld + (e - (e / ld) * ld)
-                               : wf0 + (rb + rr) * nb + e;
-      qe_cp_async(du + rr * UWmax + e, src);
-    }
-  };
-  // tasks: (state b, energy tile j) = task index b * NTB + j
-  const int n_tasks = nb * NTB;
-  double acc[kQePjTasks][4][2];
-  int tb[kQePjTasks], tj[kQePjTasks];
-  bool tv[kQePjTasks];
-#pragma unroll
-  for (int q = 0; q < kQePjTasks; ++q) {
-    const int task = warp + q * kQeMmaWarps;
-    tv[q] = task < n_tasks && (task % NTB) * 8 < NE;
-    tb[q] = task / NTB;
-    tj[q] = task % NTB;
-#pragma unroll
-    for (int mt = 0; mt < 4; ++mt) acc[q][mt][0] = acc[q][mt][1] = 0.0;
-  }
-  if (r0 < r1) issue(r0, 0);
-  qe_cp_commit();
-  int buf = 0;
-  for (int64_t rb = r0; rb < r1; rb += kQePjRows, buf ^= 1) {
-    const int nr = (int)min((int64_t)kQePjRows, r1 - rb);
-    qe_cp_wait_all();
-    __syncthreads();  // chunk rb is staged; the other buffer is consumed
-    if (rb + kQePjRows < r1) issue(rb + kQePjRows, buf ^ 1);
-    qe_cp_commit();
-    const C* cq = sq + buf * kQePjRows * QWmax;
-    const C* cu = su + buf * kQePjRows * UWmax;
-#pragma unroll
-    for (int st = 0; st < kQePjRows / 2; ++st) {
-      const int rr = 2 * st + (t >> 1);
-      const int part = t & 1;
-      const bool rok = rr < nr;
-#pragma unroll
-      for (int q = 0; q < kQePjTasks; ++q) {
-        if (!tv[q]) continue;  // warp-uniform
-        const int b = tb[q];
-        double afr[4];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-          const int mm = 8 * mt + g;
-          const int m = mm >> 1, c = mm & 1;
-          double v = 0.0;
-          if (rok && m < M) {
-            const int tau = m / K, k = m - tau * K;
-            const C w = cu[rr * UWmax + (mode == 0 ? tau * ld + k * nb + b : b)];
-            const double ur = (double)w.x, ui = (double)w.y;
-            v = c == 0 ? (part == 0 ? ur : ui) : (part == 0 ? -ui : ur);
-          }
-          afr[mt] = v;
-        }
-        const int il = tj[q] * 8 + g;  // energy within the block
-        double bv = 0.0;
-        if (rok && il < NE) {
-          const C qv = cq[rr * QWmax + il * nb + b];
-          bv = part == 0 ? (double)qv.x : (double)qv.y;
-        }
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) dmma_8x8x4(acc[q][mt][0], acc[q][mt][1], afr[mt], bv);
-      }
-    }
-  }
-  // C[mm][n]: lane holds rows mm = 8*mt + g, columns n = 2t, 2t+1 (energies)
-#pragma unroll
-  for (int q = 0; q < kQePjTasks; ++q) {
-    if (!tv[q]) continue;
-#pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-      const int mm = 8 * mt + g;
-      const int m = mm >> 1, c = mm & 1;
-      if (m >= M) continue;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int il = tj[q] * 8 + 2 * t + e;
-        if (il < NE) {
-          const int64_t o = (int64_t)m * n_ib + (int64_t)(i0 + il) * nb + tb[q];
-          partials[(o * 2 + c) * gridDim.x + blockIdx.x] = acc[q][mt][e];
-        }
-      }
-    }
-  }
-}
-
 // out[v] = sum over blocks of partials[v][block], fixed order; block per value.
 __global__ void __launch_bounds__(256) reduce_rows_kernel(const double* partials, int n_blocks,
                                                           int64_t n_values, double* out) {

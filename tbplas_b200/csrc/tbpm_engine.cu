@@ -1469,19 +1469,9 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
   // |<wf0|QE_i>| per (energy, state)
   ensure_partials(c, (size_t)2 * n_ib * pgrid);
   c->small.ensure(sizeof(double) * std::max<size_t>((size_t)2 * T2 * 2 * n_ib, 64));
-  // mma projections: blocks of qe_pj_tiles(nb) energy tiles for every state
-  const dim3 pgrid_mma((unsigned)pgrid,
-                       (unsigned)(((n_en + 7) / 8 + qe_pj_tiles(nb) - 1) / qe_pj_tiles(nb)));
-  const size_t psmem_mma = qe_pj_smem<R>(nb);
-  if (TBPM_QE_MMA) qe_smem_attr(qe_project_mma_kernel<R>, psmem_mma);
-  if (TBPM_QE_MMA)
-    qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, psmem_mma, c->stream>>>(
-        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
-        c->partials.as<double>());
-  else
-    qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(
-        qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
-        c->partials.as<double>());
+  qe_project_kernel<R><<<pgrid1, pthreads1, psmem1, c->stream>>>(
+      qe, n, rows_per_tile, n_en, nb, StatePtrs<R>{}, 1, 1, reinterpret_cast<const C*>(W),
+      c->partials.as<double>());
   TBPM_CK(cudaGetLastError());
   reduce_rows_kernel<<<(int)std::min<int64_t>(2 * n_ib, 65535), 256, 0, c->stream>>>(
       c->partials.as<double>(), pgrid, 2 * n_ib, c->small.as<double>());
@@ -1517,12 +1507,8 @@ void dc_batch(tbpm_ctx* c, const Expansion& ex_pm, const Expansion& ex_fwd, int 
       c->launches++;
       u.p[tau] = us;
     }
-    if (TBPM_QE_MMA)
-      qe_project_mma_kernel<R><<<pgrid_mma, kQeMmaWarps * 32, psmem_mma, c->stream>>>(
-          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
-    else
-      qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(
-          qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
+    qe_project_kernel<R><<<pgrid2, pthreads, psmem, c->stream>>>(
+        qe, n, rows_per_tile, n_en, nb, u, len, 0, nullptr, c->partials.as<double>());
     TBPM_CK(cudaGetLastError());
     const int64_t n_vals = (int64_t)2 * len * 2 * n_ib;
     reduce_rows_kernel<<<(int)std::min<int64_t>(n_vals, 65535), 256, 0, c->stream>>>(
