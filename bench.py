@@ -635,10 +635,10 @@ def main():
     ap.add_argument("--vector-width", type=int, default=0, choices=[0, 1, 2],
                     help="FP64 complex values per thread: 0 library default (two, 256-bit "
                          "accesses), 1 one (128-bit accesses), 2 two")
-    ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2, 3],
+    ap.add_argument("--term-kernel", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="Chebyshev-term kernel: 0 library default (shared-memory ring fed by "
                          "bulk copies), 1 grid-stride kernel with plain loads, 2 ring, 3 two "
-                         "terms per launch")
+                         "terms per launch, 4 ring with row windows")
     ap.add_argument("--threads", type=int, default=0,
                     help="FP64 threads per block of the term kernel (0: library default)")
     ap.add_argument("--nx", type=int, default=2048,

@@ -75,8 +75,10 @@ typedef struct tbpm_options {
                             2 = the ring where it applies, 3 = two terms per
                             launch (the second term of a tile after the first
                             term of every tile it couples to, p_k read back from
-                            L2) where every tile couples to at most 16 tiles;
-                            slower than the ring on the measured workloads */
+                            L2) where every tile couples to at most 16 tiles,
+                            4 = the ring with each tile's neighbour rows staged
+                            as row windows where they fit; 3 and 4 measured
+                            slower than the ring on the benchmark workload */
   double dc_budget_gb;   /* device memory (GiB) the DC driver may give its quasi-
                             eigenstate block and state ring; 0 = the free memory.
                             Fewer states per batch, then energy chunks (each

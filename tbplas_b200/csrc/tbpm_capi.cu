@@ -190,7 +190,7 @@ int tbpm_set_options(tbpm_ctx* c, const tbpm_options* o) {
   }
   if (o->batch < 0 || o->threads_per_block < 0 || o->rows_per_tile < 0 ||
       o->steps_per_graph < 0 || !(o->fp32_chk_thr >= 0) || o->vector_width < 0 ||
-      o->vector_width > 2 || o->term_kernel < 0 || o->term_kernel > 3 ||
+      o->vector_width > 2 || o->term_kernel < 0 || o->term_kernel > 4 ||
       !(o->dc_budget_gb >= 0)) {
     c->err = "negative option";
     return TBPM_ERR_ARG;

@@ -253,6 +253,7 @@ struct TermTiles {
   Tile t[3];
   bool ring[3] = {false, false, false};
   RingShape rs[3] = {};
+  const int* win = nullptr;  // window records (ring_window_kernel); null: no windows
 };
 
 // Ring layout for rows of tpr packs in kernel mode `mode` (ref_tpr: packs per
@@ -260,7 +261,7 @@ struct TermTiles {
 // ring does not apply (rows that are not a multiple of 16 bytes, or fewer than
 // two stages fit into the shared memory of one of kRingMinBlocks blocks per SM).
 template <typename R, int V>
-RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode, int ref_tpr) {
+RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode, int ref_tpr, bool win = false) {
   RingShape s{};
   const size_t row_bytes = (size_t)tpr * sizeof(Pack<R, V>);
   if (row_bytes % 16 != 0 || tpr < 1 || tpr > kRingConsumers) return s;
@@ -276,10 +277,25 @@ RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode, int ref_tpr) {
   auto al = [](size_t b) { return (int)((b + 127) & ~(size_t)127); };
   const int tile = al((size_t)TR * row_bytes);
   int off = 0;
+  s.hdr_off = -1;
+  s.win_off = -1;
+  s.win_rows = 0;
+  if (win) {
+    // window layout: the table, then rows of p_{k-1} for three tiles and a
+    // margin (graphene: its own rows and the two neighbouring rows of cells)
+    s.hdr_off = off;
+    off += kRingWinHdr;
+    s.win_rows = 3 * TR + 16;
+    s.win_off = off;
+    off += al((size_t)s.win_rows * row_bytes);
+  }
   s.pin_off = off;
   off += tile;
-  s.own_off = off;
-  off += tile;
+  s.own_off = -1;
+  if (!win) {
+    s.own_off = off;
+    off += tile;
+  }
   s.acc_off = -1;
   if (mode >= 1) {
     s.acc_off = off;
@@ -316,23 +332,61 @@ RingShape ring_shape(const tbpm_ctx* c, int tpr, int mode, int ref_tpr) {
   return s;
 }
 
-template <typename R, int V, int MODE>
+template <typename R, int V, int MODE, bool WIN>
 int ring_blocks_per_sm(const tbpm_ctx* c, const RingShape& rs) {
   static bool attr_set[64] = {false};
   const int dev = c->device;
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    TBPM_CK(cudaFuncSetAttribute(cheb_ring_kernel<R, V, MODE>,
+    TBPM_CK(cudaFuncSetAttribute(cheb_ring_kernel<R, V, MODE, WIN>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     attr_set[dev] = true;
   }
-  return resident_per_sm(cheb_ring_kernel<R, V, MODE>, kRingThreads, (size_t)rs.smem_bytes);
+  return resident_per_sm(cheb_ring_kernel<R, V, MODE, WIN>, kRingThreads, (size_t)rs.smem_bytes);
+}
+
+// The window records for tiles of `rows` rows on the current Hamiltonian,
+// built (asynchronously, on the context stream) when missing or stale; null
+// during a graph capture that finds none (recorded in c->pair_requests).
+const int* window_plan(tbpm_ctx* c, int rows) {
+  WindowPlan* p = nullptr;
+  for (auto& e : c->windows)
+    if (e->rows == rows) p = e.get();
+  if (p && p->ham_gen == c->ham.gen) return p->win.as<int>();
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TBPM_CK(cudaStreamIsCapturing(c->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    PairRequest q{};
+    q.rows = rows;
+    q.kind = 1;
+    c->pair_requests.push_back(q);
+    return nullptr;
+  }
+  if (!p) {
+    c->windows.push_back(std::make_unique<WindowPlan>());
+    p = c->windows.back().get();
+  }
+  const Ham& h = c->ham;
+  const int64_t nt = (h.n + rows - 1) / rows;
+  p->rows = rows;
+  p->ham_gen = h.gen;
+  p->n_tiles = (int)nt;
+  p->win.ensure((size_t)nt * kRingWinInts * 4);
+  p->n_gather.ensure(16);
+  TBPM_CK(cudaMemsetAsync(p->n_gather.p, 0, 4, c->stream));
+  const int grid = (int)std::min<int64_t>(blocks_for(nt, 128), (int64_t)kSMs * 16);
+  ring_window_kernel<<<grid, 128, 0, c->stream>>>(h.indptr.as<int32_t>(),
+                                                   h.indices.as<int32_t>(), h.n, rows, (int)nt,
+                                                   3 * rows + 16, p->win.as<int>(),
+                                                   p->n_gather.as<unsigned>());
+  TBPM_CK(cudaGetLastError());
+  return p->win.as<int>();
 }
 
 #ifndef TBPM_F32V4_THREADS
 #define TBPM_F32V4_THREADS 128
 #endif
 template <typename R, int V>
-TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr, int ref_tpr = 0) {
+TermTiles term_tiles(tbpm_ctx* c, int64_t n_rows, int tpr, int ref_tpr = 0) {
   TermTiles tt;
   // measured on B200 (2048^2 graphene, 16 states): 128-thread blocks for FP64,
   // 256 for FP32
@@ -340,13 +394,30 @@ TermTiles term_tiles(const tbpm_ctx* c, int64_t n_rows, int tpr, int ref_tpr = 0
   tt.t[0] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 0>, 0, th);
   tt.t[1] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 1>, 0, th);
   tt.t[2] = pick_tile(c, n_rows, tpr, cheb_term_kernel<R, V, 2>, V * 3 * sizeof(double), th);
+  // row windows (term_kernel 4) where every mode's window layout fits and the
+  // plan exists.  (Measured on B200, 2048^2 graphene, 16 states: 31.3 ms per
+  // step against 28.2 ms with gathers; each row of p_{k-1} is staged by three
+  // tiles, while the gathers of in-tile neighbours hit L1.)
+  const bool want_win = c->opts.term_kernel == 4;
+  bool win = false;
+  if (want_win && c->opts.term_kernel != 1) {
+    win = true;
+    for (int m = 0; m < 3; ++m) win = win && ring_shape<R, V>(c, tpr, m, ref_tpr, true).stages >= 2;
+    if (win) {
+      tt.win = window_plan(c, kRingConsumers / tpr);
+      win = tt.win != nullptr;
+    }
+  }
   if (c->opts.term_kernel != 1) {
     for (int m = 0; m < 3; ++m) {
-      const RingShape rs = ring_shape<R, V>(c, tpr, m, ref_tpr);
+      const RingShape rs = ring_shape<R, V>(c, tpr, m, ref_tpr, win);
       if (rs.stages == 0) continue;
-      const int per_sm = m == 0   ? ring_blocks_per_sm<R, V, 0>(c, rs)
-                         : m == 1 ? ring_blocks_per_sm<R, V, 1>(c, rs)
-                                  : ring_blocks_per_sm<R, V, 2>(c, rs);
+      const int per_sm = win ? (m == 0   ? ring_blocks_per_sm<R, V, 0, true>(c, rs)
+                                : m == 1 ? ring_blocks_per_sm<R, V, 1, true>(c, rs)
+                                         : ring_blocks_per_sm<R, V, 2, true>(c, rs))
+                             : (m == 0   ? ring_blocks_per_sm<R, V, 0, false>(c, rs)
+                                : m == 1 ? ring_blocks_per_sm<R, V, 1, false>(c, rs)
+                                         : ring_blocks_per_sm<R, V, 2, false>(c, rs));
       const int64_t tiles = (n_rows + rs.rows - 1) / rs.rows;
       Tile t;
       t.threads = kRingThreads;
@@ -372,13 +443,22 @@ int launch_term(tbpm_ctx* c, const TermTiles& tt, const TermArgs<R, V>& a) {
     ra.t = a;
     ra.s = tt.rs[mode];
     ra.status = c->status.as<unsigned int>();
+    ra.win = tt.win;
     const size_t smem = (size_t)ra.s.smem_bytes;
-    if (mode == 2)
-      cheb_ring_kernel<R, V, 2><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
-    else if (mode == 1)
-      cheb_ring_kernel<R, V, 1><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
-    else
-      cheb_ring_kernel<R, V, 0><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    if (tt.win) {
+      if (mode == 2)
+        cheb_ring_kernel<R, V, 2, true><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+      else if (mode == 1)
+        cheb_ring_kernel<R, V, 1, true><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+      else
+        cheb_ring_kernel<R, V, 0, true><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    } else if (mode == 2) {
+      cheb_ring_kernel<R, V, 2, false><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    } else if (mode == 1) {
+      cheb_ring_kernel<R, V, 1, false><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    } else {
+      cheb_ring_kernel<R, V, 0, false><<<t.grid, kRingThreads, smem, c->stream>>>(ra);
+    }
   } else if (mode == 2) {
     const size_t smem = (size_t)t.threads * V * 3 * sizeof(double);
     cheb_term_kernel<R, V, 2><<<t.grid, t.threads, smem, c->stream>>>(a);
@@ -811,7 +891,12 @@ void ensure_graph(tbpm_ctx* c, const std::vector<unsigned char>& key, Fn&& step,
     c->model_bytes = b0;
     const std::vector<PairRequest> reqs = c->pair_requests;
     c->pair_requests.clear();
-    for (const PairRequest& q : reqs) pair_plan(c, q);
+    for (const PairRequest& q : reqs) {
+      if (q.kind == 1)
+        window_plan(c, q.rows);
+      else
+        pair_plan(c, q);
+    }
   }
   c->pair_requests.clear();
   cudaError_t e = cudaGraphInstantiate(&c->graph.exec, g, 0);

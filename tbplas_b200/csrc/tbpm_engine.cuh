@@ -113,12 +113,23 @@ struct PairPlan {
   DevMem seq, deps, flags, sync;
 };
 
-// A plan asked for while a graph was being captured (it cannot be built
-// then: the build synchronises); ensure_graph builds it and captures again.
+// Row windows of the ring kernels (ring_window_kernel) for one tile height on
+// the current Hamiltonian (gen).
+struct WindowPlan {
+  int rows = 0;
+  uint64_t ham_gen = 0;
+  int n_tiles = 0;
+  DevMem win, n_gather;
+};
+
+// A plan asked for while a graph was being captured (its build launches
+// kernels outside the graph, and the pair plan synchronises); ensure_graph
+// builds it and captures again.  kind 0: pair plan, 1: window plan (rows only).
 struct PairRequest {
   int rows, grid, stages;
   size_t tile_bytes;
   bool force;
+  int kind = 0;
 };
 
 struct Session {
@@ -144,6 +155,7 @@ struct tbpm_ctx {
   tbpm::DevMem status;  // bit 0: a bounded device-side wait ran out (cleared when read)
   tbpm::DevMem anl;     // inputs and outputs of the Analyzer's trigonometric sums
   std::vector<std::unique_ptr<tbpm::PairPlan>> pairs;  // paired-term plans, by tile height
+  std::vector<std::unique_ptr<tbpm::WindowPlan>> windows;  // ring window plans, by tile height
   std::vector<tbpm::PairRequest> pair_requests;
   tbpm::DevMem pair_tmp;  // scratch of the plan build
   int64_t launches = 0;

@@ -78,6 +78,9 @@ struct RingShape {
   int stages;       // S
   int cap;          // CSR entries a stage holds (multiple of 4)
   int pin_off, own_off, acc_off, diag_off, ip_off, ix_off, hop_off;
+  int hdr_off;      // window layouts: the stage's window table (kRingWinHdr bytes)
+  int win_off;      // window layouts: rows of p_{k-1} covering the tile's columns
+  int win_rows;     // window layouts: rows the window region holds
   int ref_off;      // MODE 2: rows of the correlation reference (-1: read from global)
   int stage_bytes;  // one stage
   int bar_off;      // 2*S mbarriers (full[S], empty[S]) after the stages
@@ -89,7 +92,20 @@ struct RingArgs {
   TermArgs<R, V> t;
   RingShape s;
   unsigned int* status;  // bit 0: a bounded wait ran out
+  const int* win;        // WIN kernels: per tile kRingWinInts ints (ring_window_kernel)
 };
+
+// Row windows (the WIN kernels): a tile's off-diagonal columns and its own
+// rows are covered by at most kRingWinMax row ranges of p_{k-1}, staged into
+// the stage's window region by bulk copies; the consumers read every operand
+// from shared memory.  Record per tile: [0] = number of windows | (gather
+// flag << 8), then (first row, row count) per window.  A tile whose columns do
+// not fit (more windows, or more rows than the region) stages its own rows as
+// its one window and gathers the neighbours from global memory.
+constexpr int kRingWinMax = 4;
+constexpr int kRingWinInts = 12;   // record size (3 x int4)
+constexpr int kRingWinHdr = 64;    // stage table: flags, lo[4], base[4]
+constexpr int kRingWinGap = 8;     // rows between two column runs merged into one window
 
 __device__ __forceinline__ uint32_t ring_smem(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -164,7 +180,7 @@ __device__ __forceinline__ Pack<R, V> lds_pack(const char* p) {
   return *reinterpret_cast<const Pack<R, V>*>(p);
 }
 
-template <typename R, int V, int MODE>
+template <typename R, int V, int MODE, bool WIN>
 __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     cheb_ring_kernel(const __grid_constant__ RingArgs<R, V> ra) {
   using C = typename Cx<R>::t;
@@ -218,6 +234,23 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
     int cur0, cur1, nxt0, nxt1;
     bounds(wl, &cur0, &cur1);
     bounds(32 + wl, &nxt0, &nxt1);
+    // WIN: the window records of the same tiles
+    auto record = [&](int64_t i, int4* w) {
+      const int64_t t = (int64_t)blockIdx.x + i * gridDim.x;
+      if (WIN && t * TR < n) {
+        const int4* p = reinterpret_cast<const int4*>(ra.win + t * kRingWinInts);
+        w[0] = p[0];
+        w[1] = p[1];
+        w[2] = p[2];
+      } else {
+        w[0] = w[1] = w[2] = make_int4(0, 0, 0, 0);
+      }
+    };
+    int4 wcur[3], wnxt[3];
+    if (WIN) {
+      record(wl, wcur);
+      record(32 + wl, wnxt);
+    }
     for (int64_t i = 0;; ++i) {
       const int64_t r0 = ((int64_t)blockIdx.x + i * gridDim.x) * TR;
       if (r0 >= n) break;
@@ -225,6 +258,25 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
         cur0 = nxt0;
         cur1 = nxt1;
         bounds(i + 32 + wl, &nxt0, &nxt1);
+        if (WIN) {
+          wcur[0] = wnxt[0];
+          wcur[1] = wnxt[1];
+          wcur[2] = wnxt[2];
+          record(i + 32 + wl, wnxt);
+        }
+      }
+      int wr[9];
+      if (WIN) {
+        const int src = (int)(i & 31);
+        wr[0] = __shfl_sync(0xffffffffu, wcur[0].x, src);
+        wr[1] = __shfl_sync(0xffffffffu, wcur[0].y, src);
+        wr[2] = __shfl_sync(0xffffffffu, wcur[0].z, src);
+        wr[3] = __shfl_sync(0xffffffffu, wcur[0].w, src);
+        wr[4] = __shfl_sync(0xffffffffu, wcur[1].x, src);
+        wr[5] = __shfl_sync(0xffffffffu, wcur[1].y, src);
+        wr[6] = __shfl_sync(0xffffffffu, wcur[1].z, src);
+        wr[7] = __shfl_sync(0xffffffffu, wcur[1].w, src);
+        wr[8] = __shfl_sync(0xffffffffu, wcur[2].x, src);
       }
       const int j0 = __shfl_sync(0xffffffffu, cur0, (int)(i & 31));
       const int j1 = __shfl_sync(0xffffffffu, cur1, (int)(i & 31));
@@ -260,9 +312,26 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
         const uint32_t tile = (uint32_t)(nr * row_bytes);
         const uint32_t ref_tile = (uint32_t)(nr * a.ref_tpr * (int64_t)sizeof(Pack<R, V>));
         if (a.pin) bytes += tile;
-        if (need_own) bytes += tile;
+        if (need_own && !WIN) bytes += tile;
         if (add_acc) bytes += tile;
         if (ref_staged) bytes += ref_tile;
+        int n_w = 0;
+        if (WIN) {
+          // the stage's window table: lo[w] and base[w] = (row offset in the
+          // region) - lo[w], so a column c of window w sits at row base[w] + c
+          int* hdr = reinterpret_cast<int*>(st + sh.hdr_off);
+          n_w = wr[0] & 0xff;
+          int off = 0;
+#pragma unroll
+          for (int w = 0; w < kRingWinMax; ++w) {
+            const int lo = wr[1 + 2 * w], len = wr[2 + 2 * w];
+            hdr[1 + w] = w < n_w ? lo : 0x7fffffff;
+            hdr[5 + w] = w < n_w ? off - lo : 0;
+            if (w < n_w) off += len;
+          }
+          hdr[0] = wr[0];
+          bytes += (uint32_t)(off * row_bytes);
+        }
         ring_arrive_tx(bar, bytes);
         ring_copy(ring_smem(st + sh.ip_off), a.indptr + r0a, ip_bytes, bar);
         if (csr_in) {
@@ -280,7 +349,19 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           if (a.pin) ring_copy(ring_smem(st + sh.pin_off), a.pin + e0, tile, bar);
           if (add_acc) ring_copy(ring_smem(st + sh.acc_off), a.acc + e0, tile, bar);
         }
-        if (need_own) ring_copy(ring_smem(st + sh.own_off), a.gather + e0, tile, bar);
+        if (need_own && !WIN) ring_copy(ring_smem(st + sh.own_off), a.gather + e0, tile, bar);
+        if (WIN) {
+          int off = 0;
+#pragma unroll
+          for (int w = 0; w < kRingWinMax; ++w) {
+            const int lo = wr[1 + 2 * w], len = wr[2 + 2 * w];
+            if (w < n_w) {
+              ring_copy(ring_smem(st + sh.win_off + (int64_t)off * row_bytes),
+                        a.gather + (int64_t)lo * tpr, (uint32_t)(len * row_bytes), bar);
+              off += len;
+            }
+          }
+        }
         if (ref_staged)
           ring_copy(ring_smem(st + sh.ref_off), a.ref + r0 * a.ref_tpr, ref_tile, bar);
       }
@@ -323,6 +404,17 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
         const bool csr_in = cnt > 0 && cnt <= sh.cap;
         const int32_t* ixs = reinterpret_cast<const int32_t*>(st + sh.ix_off) - ja;
         const C* hs = reinterpret_cast<const C*>(st + sh.hop_off) - ja;
+        // WIN: row of column c in the window region (windows sorted by lo)
+        const int* hdr = reinterpret_cast<const int*>(st + sh.hdr_off);
+        const bool wgat = !WIN || ((hdr[0] >> 8) & 1);
+        auto wrow = [&](int col) -> int64_t {
+          int b = hdr[5];
+          if (col >= hdr[2]) b = hdr[6];
+          if (col >= hdr[3]) b = hdr[7];
+          if (col >= hdr[4]) b = hdr[8];
+          return (int64_t)b + col;
+        };
+        const char* wreg = st + sh.win_off;
         const int64_t e = r * tpr + lane;
         const int64_t te = (int64_t)slot * tpr + lane;  // pack index within the tile
         R sre[V], sim[V];
@@ -346,7 +438,9 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
             if (cidx[u] >= 0) {
               // neighbours inside the tile come from its staged rows of p_{k-1}
               const int64_t lc = (int64_t)cidx[u] - r0;
-              if (TBPM_RING_LOCAL && need_own && lc >= 0 && lc < nr)
+              if (WIN && !wgat)
+                x[u] = lds_pack<R, V>(wreg + (wrow(cidx[u]) * tpr + lane) * sizeof(Pack<R, V>));
+              else if (!WIN && TBPM_RING_LOCAL && need_own && lc >= 0 && lc < nr)
                 x[u] = lds_pack<R, V>(st + sh.own_off + (lc * tpr + lane) * sizeof(Pack<R, V>));
               else
                 x[u] = ldg_pack(a.gather + (int64_t)cidx[u] * tpr + lane);
@@ -354,7 +448,9 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
           if (first) {
             // staged operands while the gathers are in flight: sum = D p_{k-1}
             first = false;
-            if (need_own) own = lds_pack<R, V>(st + sh.own_off + te * sizeof(Pack<R, V>));
+            if (need_own)
+              own = WIN ? lds_pack<R, V>(wreg + (wrow((int)r) * tpr + lane) * sizeof(Pack<R, V>))
+                        : lds_pack<R, V>(st + sh.own_off + te * sizeof(Pack<R, V>));
             if (a.diag) {
               constexpr int al = 16 / (int)sizeof(C);
               const C d = reinterpret_cast<const C*>(st + sh.diag_off)[r - (r0 - r0 % al)];
@@ -466,6 +562,81 @@ __global__ void __launch_bounds__(kRingThreads, kRingMinBlocks)
         for (int q = 0; q < 3; ++q)
           a.partials[(int64_t)(col * 3 + q) * gridDim.x + blockIdx.x] = red[col * 3 + q];
       }
+    }
+  }
+}
+
+// ---- window plan ----------------------------------------------------------
+
+// One thread per tile of TR rows: cover its own rows and the columns of its
+// off-diagonal entries with row ranges, merging runs closer than kRingWinGap
+// rows; at most kRingWinMax ranges and `budget` rows in total, else the tile
+// is marked for global gathers with its own rows as its one window.
+__global__ void ring_window_kernel(const int32_t* __restrict__ indptr,
+                                   const int32_t* __restrict__ indices, int64_t n, int TR,
+                                   int n_tiles, int budget, int* win, unsigned* n_gather) {
+  constexpr int K = 8;  // runs tracked before the merge
+  for (int T = blockIdx.x * blockDim.x + threadIdx.x; T < n_tiles; T += gridDim.x * blockDim.x) {
+    const int64_t r0 = (int64_t)T * TR;
+    const int64_t r1 = r0 + TR < n ? r0 + TR : n;
+    int lo[K], hi[K];  // [lo, hi)
+    int m = 1;
+    lo[0] = (int)r0;
+    hi[0] = (int)r1;
+    bool over = false;
+    const int j1 = indptr[r1];
+    for (int j = indptr[r0]; j < j1 && !over; ++j) {
+      const int c = indices[j];
+      int k = 0;
+      for (; k < m; ++k)
+        if (c >= lo[k] - kRingWinGap && c < hi[k] + kRingWinGap) break;
+      if (k < m) {
+        lo[k] = c < lo[k] ? c : lo[k];
+        hi[k] = c + 1 > hi[k] ? c + 1 : hi[k];
+      } else if (m < K) {
+        lo[m] = c;
+        hi[m] = c + 1;
+        ++m;
+      } else {
+        over = true;
+      }
+    }
+    // sort by lo, then merge runs that overlap or lie within the gap
+    for (int a = 1; a < m; ++a)
+      for (int b = a; b > 0 && lo[b] < lo[b - 1]; --b) {
+        const int tl = lo[b], th = hi[b];
+        lo[b] = lo[b - 1];
+        hi[b] = hi[b - 1];
+        lo[b - 1] = tl;
+        hi[b - 1] = th;
+      }
+    int q = 0;
+    for (int a = 1; a < m; ++a) {
+      if (lo[a] <= hi[q] + kRingWinGap) {
+        hi[q] = hi[a] > hi[q] ? hi[a] : hi[q];
+      } else {
+        ++q;
+        lo[q] = lo[a];
+        hi[q] = hi[a];
+      }
+    }
+    const int nw = q + 1;
+    int rows = 0;
+    for (int a = 0; a < nw; ++a) rows += hi[a] - lo[a];
+    int* rec = win + (int64_t)T * kRingWinInts;
+    if (over || nw > kRingWinMax || rows > budget) {
+      rec[0] = 1 | (1 << 8);
+      rec[1] = (int)r0;
+      rec[2] = (int)(r1 - r0);
+      for (int a = 3; a < kRingWinInts; ++a) rec[a] = 0;
+      atomicAdd(n_gather, 1u);
+    } else {
+      rec[0] = nw;
+      for (int a = 0; a < kRingWinMax; ++a) {
+        rec[1 + 2 * a] = a < nw ? lo[a] : 0;
+        rec[2 + 2 * a] = a < nw ? hi[a] - lo[a] : 0;
+      }
+      for (int a = 1 + 2 * kRingWinMax; a < kRingWinInts; ++a) rec[a] = 0;
     }
   }
 }
