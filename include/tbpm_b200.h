@@ -70,7 +70,8 @@ typedef struct tbpm_options {
                             block width allows), 1 = one (128-bit accesses), 2 */
   int term_kernel;       /* Chebyshev-term kernel: 0 = automatic (the shared-memory
                             ring fed by bulk copies wherever a row of the state
-                            block is a multiple of 16 bytes, else the grid-stride
+                            block is a multiple of 16 bytes and the rows make at
+                            least two ring tiles per SM, else the grid-stride
                             kernel), 1 = the grid-stride kernel with plain loads,
                             2 = the ring where it applies, 3 = two terms per
                             launch (the second term of a tile after the first

@@ -408,7 +408,14 @@ TermTiles term_tiles(tbpm_ctx* c, int64_t n_rows, int tpr, int ref_tpr = 0) {
       win = tt.win != nullptr;
     }
   }
-  if (c->opts.term_kernel != 1) {
+  // the automatic choice keeps small problems (fewer than two ring tiles per
+  // SM) on the grid-stride kernel, whose smaller tiles spread them over more
+  // SMs (measured on B200: 100^2 graphene, one state, 256 steps, 16 ms against
+  // 21 ms with the ring)
+  const bool small = c->opts.term_kernel == 0 && tpr <= kRingConsumers &&
+                     (n_rows + kRingConsumers / tpr - 1) / (kRingConsumers / tpr) <
+                         2 * (int64_t)num_sms(c->device);
+  if (c->opts.term_kernel != 1 && !small) {
     for (int m = 0; m < 3; ++m) {
       const RingShape rs = ring_shape<R, V>(c, tpr, m, ref_tpr, win);
       if (rs.stages == 0) continue;

@@ -213,17 +213,22 @@ def test_ring_kernel_with_a_dense_row(graphene_small):
     hv = np.array(vals, dtype=np.complex128)
     wf0 = unit_states(16, n, seed=8)
     bes = bessel_series(math.pi)
+    f2py.set_backend(term_kernel=2)  # the ring kernel at this small size
     got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 12, 128, 1e-9)
+    f2py.set_backend(term_kernel=0)
     ref = oracle.tbpm_dos(bes, ip, ix, hv, 12, wf0=wf0)
     assert rel_err(got, ref) < FP64_TOL
 
 
+@pytest.mark.parametrize("kernel", [0, 2])
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
 @pytest.mark.parametrize("case", ["dimer", "chain5", "diagonal_only", "one_row"])
-def test_tiny_and_degenerate_hamiltonians(prec, tol, case):
+def test_tiny_and_degenerate_hamiltonians(prec, tol, case, kernel):
     """Fewer rows than one tile of the ring kernel (60 rows at 16 states), row
     counts that are not multiples of 4 (the widened indptr window), no
-    off-diagonal entries at all (no CSR slice to stage), and a single row."""
+    off-diagonal entries at all (no CSR slice to stage), and a single row;
+    through the ring kernel (term_kernel 2) and the automatic choice (which
+    takes the grid-stride kernel at these sizes)."""
     if case == "dimer":
         n, rows = 2, {0: [(1, -0.4)], 1: [(0, -0.4)]}
     elif case == "chain5":
@@ -247,8 +252,9 @@ def test_tiny_and_degenerate_hamiltonians(prec, tol, case):
     hv = np.array(hv, dtype=np.complex128)
     wf0 = unit_states(16, n, seed=3)
     bes = bessel_series(math.pi)
-    f2py.set_backend(precision=prec)
+    f2py.set_backend(precision=prec, term_kernel=kernel)
     got = f2py.tbpm_dos_states(bes, ip, ix, hv, wf0, 20, 8, 1e-9)
+    f2py.set_backend(term_kernel=0)
     ref = oracle.tbpm_dos(bes, ip, ix, hv, 20, wf0=wf0)
     assert rel_err(got, ref) < tol
 
