@@ -504,7 +504,13 @@ __global__ void __launch_bounds__(512) current_apply_kernel(
 //   <psi2|J_x psi1_x>, <psi2|J_y psi1_x>, <psi2|J_x psi1_y>, <psi2|J_y psi1_y>
 // and <psi2|psi2>; partials [(b*9 + v) * grid + block], v = re/im pairs then norm.
 template <typename R>
-__global__ void __launch_bounds__(512) jcorr_kernel(
+#ifndef TBPM_JCORR_JB
+#define TBPM_JCORR_JB 4  // neighbour entries whose loads are issued together
+#endif
+#ifndef TBPM_JCORR_MINB
+#define TBPM_JCORR_MINB 2  // resident 256-thread blocks per SM the registers are bounded for
+#endif
+__global__ void __launch_bounds__(256, TBPM_JCORR_MINB) jcorr_kernel(
     const int32_t* indptr, const int32_t* indices, const typename Cx<R>::t* hop,
     const R* dx, const R* dy, double rescale, int64_t n_rows, int64_t rows_per_tile, int B,
     const typename Cx<R>::t* psi, double* partials) {
@@ -526,7 +532,7 @@ __global__ void __launch_bounds__(512) jcorr_kernel(
     const typename Cx<R>::t p2 = ldg_c(psi + r * ld + 2 * B + b);
     // neighbours in batches of JB: every load of a batch is issued before the
     // first product, so the gathers overlap (the products keep the entry order)
-    constexpr int JB = 4;
+    constexpr int JB = TBPM_JCORR_JB;
     for (int jb = j0; jb < j1; jb += JB) {
       int cc[JB];
       typename Cx<R>::t hh[JB];
