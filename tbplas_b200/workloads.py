@@ -252,20 +252,43 @@ def _pack(parts):
         np.array(offsets, dtype=np.int64)
 
 
+def _field_realisation(args):
+    nx, ny, w, b_field, seed = args
+    s = make_graphene_sample(nx, ny, disorder=w, rescale=9.0, seed=seed)
+    s.set_magnetic_field(b_field, gauge=0)
+    h = s.build_ham_csr()
+    return h.indptr.astype(np.int64), h.indices.astype(np.int32), h.data
+
+
+def _curves_from_parts(parts, n_states: int, tnr: int, precision: str, seed: int):
+    """Per-state DOS correlations of the realisations in `parts` (CSR arrays),
+    packed into one launch; returns them and the GPU seconds spent."""
+    bes = bessel_series(math.pi)
+    ip, ix, hv, off = _pack(parts)
+    try:
+        f2py.set_backend(precision=precision)
+        (corr, per), sec = _timed(lambda: f2py.tbpm_dos_segmented(
+            bes, ip, ix, hv, off, n_states, seed, tnr, per_state=True))
+    finally:
+        f2py.set_backend(precision="fp64")
+    return per, sec
+
+
 def generate_curves(specs, n_states: int, tnr: int, precision: str, seed: int,
-                    pack: int = 16, workers=None):
+                    pack: int = 16, workers=None, build=None):
     """Per-state DOS correlations of graphene realisations specs = [(nx, ny,
-    W, vacancy_rate, seed)], propagated on the GPU in packs of `pack`
-    realisations.  Returns (n_real, n_states, tnr+1) complex128 and the GPU
-    seconds spent."""
+    W, vacancy_rate, seed)] (or the arguments of `build`), propagated on the
+    GPU in packs of `pack` realisations.  Returns (n_real, n_states, tnr+1)
+    complex128 and the GPU seconds spent."""
     import concurrent.futures as cf
     import multiprocessing as mp
     workers = workers or min(8, os.cpu_count() or 1)
     out, gpu_sec = [], 0.0
     bes = bessel_series(math.pi)  # dt*rescale = pi for rescale 10 and dt = 2 pi / 20
+    build = build or _realisation
     with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
         for p0 in range(0, len(specs), pack):
-            parts = list(ex.map(_realisation, specs[p0:p0 + pack]))
+            parts = list(ex.map(build, specs[p0:p0 + pack]))
             ip, ix, hv, off = _pack(parts)
             f2py.set_backend(precision=precision)
             (corr, per), sec = _timed(lambda: f2py.tbpm_dos_segmented(
@@ -277,6 +300,7 @@ def generate_curves(specs, n_states: int, tnr: int, precision: str, seed: int,
 
 
 def _l1_mean(curves, refs, e_range: float = 20.0) -> float:
+    # e_range: the energy range 2 * rescale of the samples (10 eV for c4)
     from .learned import dos_l1 as l1
     return float(np.mean([l1(curves[k], refs[k], e_range) for k in range(len(refs))]))
 
@@ -516,8 +540,87 @@ def run_c4l(**kw) -> dict:
     return run_c4c(**args)
 
 
+def run_c5l(n_train: int = 64, nx_train: int = 1024, nx_test: int = 4096, n_states: int = 8,
+            tnr: int = 2048, n_in: int = 256, epochs: int = 200, seed: int = 2025,
+            target_l1: float = 1e-3) -> dict:
+    """Configuration 5's plain vs learned-tail comparison, for the DOS: the
+    tail network is trained on FP32 C(t) of nx_train^2 graphene in the same
+    field (h/e per 1024 hexagons, 77.06 T) and disorder (W = 1 eV), then
+    applied to the first n_in FP32 steps of a 4096^2 realisation and compared
+    with plain FP64 propagation of the same states (DOS L1 against the full
+    tnr-step FP64 curve).  Seconds per path scale the full runs' per-step
+    times."""
+    from .learned import TailNet, curves_to_xy, extend
+    flux_quantum = 4135.667  # h/e in T nm^2
+    b_field = flux_quantum / (1024 * LatticeSample((1, 1)).area_unit_cell)
+    e_range = 18.0  # 2 * rescale
+    res = {"workload": f"c5 learned tail (DOS): train {n_train} x {nx_train}^2, test {nx_test}^2, "
+                       f"B={b_field:.2f} T, W=1 eV, {n_states} states, n_in={n_in} -> {tnr}",
+           "n_train_curves": n_train * n_states, "target_l1": target_l1}
+    train_specs = [(nx_train, nx_train, 1.0, b_field, 30_000 + i) for i in range(n_train)]
+    train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1, pack=8,
+                                   build=_field_realisation)
+    res["datagen_gpu_seconds"] = t_gen
+    parts, t_build = _timed(lambda: [_field_realisation((nx_test, nx_test, 1.0, b_field, 1337))])
+    res["test_host_build_seconds"] = t_build
+    ev64, t64 = _curves_from_parts(parts, n_states, tnr, "fp64", 7)
+    ev32, t32 = _curves_from_parts(parts, n_states, tnr, "fp32", 7)
+    res["test_fp64_seconds"] = t64
+    res["test_fp32_seconds"] = t32
+    c64, c32 = ev64.mean(axis=1), ev32.mean(axis=1)
+    grid = (128, 256, 384, 512, 768, 1024, 1536, 1792, 1920, tnr)
+    same64 = {n: _l1_mean(c64[:, :n + 1], c64, e_range) for n in grid}
+    same32 = {n: _l1_mean(c32[:, :n + 1], c64, e_range) for n in grid}
+    res["l1_same_states_plain_fp64"] = {str(k): v for k, v in same64.items()}
+    res["l1_same_states_fp32"] = {str(k): v for k, v in same32.items()}
+    best = None
+    for name, targets in (("per_state", "state"), ("state_mean", "mean")):
+        src = train.reshape(-1, tnr + 1) if targets == "state" else train.mean(axis=1)
+        x, y = curves_to_xy(src.astype(np.complex128), n_in, tnr - n_in)
+        n_val = max(8, len(x) // 8)
+        net = TailNet(n_in=n_in, n_out=tnr - n_in, seed=seed)
+        net.fit_scales(x, y)
+        hist, t_train = _timed(lambda: net.train(x[n_val:], y[n_val:], epochs=epochs, batch=64,
+                                                 lr=1e-3, weight_decay=1e-2, x_val=x[:n_val],
+                                                 y_val=y[:n_val], patience=30))
+        if targets == "state":
+            xs, _ = curves_to_xy(ev32.reshape(-1, tnr + 1), n_in, tnr - n_in)
+            tail = net.predict(xs).reshape(1, n_states, tnr - n_in, 2).mean(axis=1)
+        else:
+            xs, _ = curves_to_xy(c32, n_in, tnr - n_in)
+            tail = net.predict(xs)
+        learned = extend(c32[:, :n_in + 1], tail)
+        r = {"train_seconds": t_train, "best_epoch": hist["best_epoch"],
+             "val_mse_initial": hist.get("val_initial"), "val_mse_best": hist.get("val_best"),
+             "l1_same_states": _l1_mean(learned, c64, e_range)}
+        res[f"variant_{name}"] = r
+        if best is None or r["l1_same_states"] < best[1]["l1_same_states"]:
+            best = (name, r)
+    res["best_variant"] = best[0]
+    res["l1_same_states_learned"] = best[1]["l1_same_states"]
+    res["l1_same_states_truncated_at_n_in_fp32"] = same32[n_in]
+    zero = np.zeros((1, tnr - n_in, 2))
+    res["l1_same_states_zero_tail_fp32"] = _l1_mean(extend(c32[:, :n_in + 1], zero), c64,
+                                                    e_range)
+    n64 = _steps_to_reach(same64, target_l1)
+    n32 = _steps_to_reach(same32, target_l1)
+    learned_ok = best[1]["l1_same_states"] < target_l1
+    per64, per32 = t64 / tnr, t32 / tnr
+    res["time_to_dos"] = {
+        "plain_fp64": {"steps": n64, "seconds": n64 * per64 if n64 else None},
+        "fp32": {"steps": n32, "seconds": n32 * per32 if n32 else None},
+        "fp32_learned": {"reached": learned_ok, "steps": n_in if learned_ok else None,
+                         "seconds": n_in * per32 if learned_ok else None},
+    }
+    if n64 and learned_ok:
+        res["time_to_dos_speedup_learned_vs_plain_fp64"] = (n64 * per64) / (n_in * per32)
+    if n64 and n32:
+        res["time_to_dos_speedup_fp32_vs_plain_fp64"] = (n64 * per64) / (n32 * per32)
+    return res
+
+
 RUNNERS = {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c4c": run_c4c, "c4l": run_c4l,
-           "c5": run_c5}
+           "c5": run_c5, "c5l": run_c5l}
 
 
 def main(argv=None) -> None:
@@ -541,7 +644,9 @@ def main(argv=None) -> None:
     args = ap.parse_args(argv)
     for w in args.workloads:
         kw = {}
-        if args.steps:
+        if w == "c5l" and args.n_train:
+            kw["n_train"] = args.n_train
+        if args.steps and w != "c5l":
             kw = {"steps": args.steps} if w in ("c1", "c3", "c5") else \
                  {"steps_dos": args.steps, "steps_ac": args.steps}
         if w == "c4" and args.data:
