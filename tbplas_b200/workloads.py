@@ -542,14 +542,14 @@ def run_c4l(**kw) -> dict:
 
 def run_c5l(n_train: int = 64, nx_train: int = 1024, nx_test: int = 4096, n_states: int = 8,
             tnr: int = 2048, n_in: int = 256, epochs: int = 200, seed: int = 2025,
-            target_l1: float = 1e-3) -> dict:
+            target_l1: float = 1e-3, data: str = None) -> dict:
     """Configuration 5's plain vs learned-tail comparison, for the DOS: the
     tail network is trained on FP32 C(t) of nx_train^2 graphene in the same
     field (h/e per 1024 hexagons, 77.06 T) and disorder (W = 1 eV), then
     applied to the first n_in FP32 steps of a 4096^2 realisation and compared
     with plain FP64 propagation of the same states (DOS L1 against the full
     tnr-step FP64 curve).  Seconds per path scale the full runs' per-step
-    times."""
+    times.  `data`: npz cache of the generated curves (written when absent)."""
     from .learned import TailNet, curves_to_xy, extend
     flux_quantum = 4135.667  # h/e in T nm^2
     b_field = flux_quantum / (1024 * LatticeSample((1, 1)).area_unit_cell)
@@ -557,14 +557,24 @@ def run_c5l(n_train: int = 64, nx_train: int = 1024, nx_test: int = 4096, n_stat
     res = {"workload": f"c5 learned tail (DOS): train {n_train} x {nx_train}^2, test {nx_test}^2, "
                        f"B={b_field:.2f} T, W=1 eV, {n_states} states, n_in={n_in} -> {tnr}",
            "n_train_curves": n_train * n_states, "target_l1": target_l1}
-    train_specs = [(nx_train, nx_train, 1.0, b_field, 30_000 + i) for i in range(n_train)]
-    train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1, pack=8,
-                                   build=_field_realisation)
+    if data and os.path.exists(data):
+        d = np.load(data)
+        train, ev64, ev32 = d["train"], d["ev64"], d["ev32"]
+        t_gen, t64, t32 = float(d["t_gen"]), float(d["t64"]), float(d["t32"])
+    else:
+        train_specs = [(nx_train, nx_train, 1.0, b_field, 30_000 + i) for i in range(n_train)]
+        train, t_gen = generate_curves(train_specs, n_states, tnr, "fp32", 1, pack=8,
+                                       build=_field_realisation)
+        parts, t_build = _timed(
+            lambda: [_field_realisation((nx_test, nx_test, 1.0, b_field, 1337))])
+        res["test_host_build_seconds"] = t_build
+        ev64, t64 = _curves_from_parts(parts, n_states, tnr, "fp64", 7)
+        ev32, t32 = _curves_from_parts(parts, n_states, tnr, "fp32", 7)
+        if data:
+            np.savez(data, train=train.astype(np.complex64), ev64=ev64, ev32=ev32, t_gen=t_gen,
+                     t64=t64, t32=t32)
+    res["n_train_curves"] = int(train.shape[0] * train.shape[1])
     res["datagen_gpu_seconds"] = t_gen
-    parts, t_build = _timed(lambda: [_field_realisation((nx_test, nx_test, 1.0, b_field, 1337))])
-    res["test_host_build_seconds"] = t_build
-    ev64, t64 = _curves_from_parts(parts, n_states, tnr, "fp64", 7)
-    ev32, t32 = _curves_from_parts(parts, n_states, tnr, "fp32", 7)
     res["test_fp64_seconds"] = t64
     res["test_fp32_seconds"] = t32
     c64, c32 = ev64.mean(axis=1), ev32.mean(axis=1)
@@ -577,7 +587,7 @@ def run_c5l(n_train: int = 64, nx_train: int = 1024, nx_test: int = 4096, n_stat
     for name, targets in (("per_state", "state"), ("state_mean", "mean")):
         src = train.reshape(-1, tnr + 1) if targets == "state" else train.mean(axis=1)
         x, y = curves_to_xy(src.astype(np.complex128), n_in, tnr - n_in)
-        n_val = max(8, len(x) // 8)
+        n_val = max(2, len(x) // 8)  # validation curves (the mean targets are few)
         net = TailNet(n_in=n_in, n_out=tnr - n_in, seed=seed)
         net.fit_scales(x, y)
         hist, t_train = _timed(lambda: net.train(x[n_val:], y[n_val:], epochs=epochs, batch=64,
@@ -629,7 +639,8 @@ def main(argv=None) -> None:
     ap.add_argument("--steps", type=int, default=None,
                     help="override the number of time steps (shorter runs)")
     ap.add_argument("--out", default=None)
-    ap.add_argument("--data", default=None, help="c4: npz cache of the generated curves")
+    ap.add_argument("--data", default=None, help="c4, c5l: npz cache of the generated curves")
+    ap.add_argument("--epochs", type=int, default=None, help="c4, c5l: training epochs")
     ap.add_argument("--n-train", type=int, default=None,
                     help="c4: training realisations (curves = realisations x states)")
     ap.add_argument("--n-states", type=int, default=None,
@@ -646,6 +657,10 @@ def main(argv=None) -> None:
         kw = {}
         if w == "c5l" and args.n_train:
             kw["n_train"] = args.n_train
+        if w in ("c4", "c5l") and args.epochs:
+            kw["epochs"] = args.epochs
+        if w == "c5l" and args.data:
+            kw["data"] = args.data
         if args.steps and w != "c5l":
             kw = {"steps": args.steps} if w in ("c1", "c3", "c5") else \
                  {"steps_dos": args.steps, "steps_ac": args.steps}
