@@ -27,7 +27,6 @@ import time
 
 import numpy as np
 
-from . import _native as nat
 from .builder import LatticeSample, make_graphene_sample
 from .fortran import f2py
 from .tbpm import Analyzer, Config, Solver
